@@ -1,0 +1,105 @@
+// Shared definitions for the PHOENIX-B200 raymarch path: host/device qualifiers, constants and a few math helpers
+// that have a cheaper device form.  The same headers are compiled by nvcc (device kernels, host set-up) and by g++
+// (host tools such as the snapshot generator and the dump reader).
+#pragma once
+
+#include <cmath>
+#include <cstddef>
+#include <cstdint>
+
+#if defined(__CUDACC__)
+#define PHX_HD __host__ __device__ __forceinline__
+#define PHX_D __device__ __forceinline__
+#else
+#define PHX_HD inline
+#define PHX_D inline
+#endif
+
+namespace phx {
+
+constexpr double kPi = 3.14159265358979323846264338327950288;
+constexpr double kTwoPi = 2.0 * kPi;
+constexpr double kHalfPi = 0.5 * kPi;
+
+// CGS constants.  These are the CODATA-era values the reference renderer uses (core/numerics/constants.hpp:22-52);
+// the flux of an image scales with them, so they have to be the same numbers for results to agree.
+namespace cgs {
+constexpr double m_proton = 1.6726219e-24;
+constexpr double m_electron = 9.1093829e-28;
+constexpr double q_electron = 4.80320425e-10;
+constexpr double k_boltzmann = 1.3806488e-16;
+constexpr double c_light = 2.99792458e10;
+constexpr double h_planck = 6.62606885e-27;
+constexpr double g_newton = 6.674e-8;
+constexpr double m_sun = 1.989e33;
+constexpr double kpc = 3.086e21;
+constexpr double jansky = 1e23;
+}  // namespace cgs
+
+// Maximum number of AMR levels a snapshot may carry (the level table of the reference model is 16 deep).
+constexpr int kMaxLevels = 16;
+// Maximum number of observing frequencies in one render (the reference's CPU default for PHX_MAX_FREQS).
+constexpr int kMaxFreqs = 32;
+// Primitive slots of one cell, RAPTOR order: rho, u, u^1..3 (Lorentz factor times 3-velocity), B^1..3.
+enum Prim { kRho = 0, kUU = 1, kU1 = 2, kU2 = 3, kU3 = 4, kB1 = 5, kB2 = 6, kB3 = 7, kNPrim = 8 };
+
+template <class T>
+PHX_HD void sincos_t(T x, T* s, T* c) {
+#if defined(__CUDA_ARCH__)
+  if constexpr (sizeof(T) == 4) {
+    sincosf(x, s, c);
+  } else {
+    sincos(x, s, c);
+  }
+#else
+  *s = std::sin(x);
+  *c = std::cos(x);
+#endif
+}
+
+// x mod y for y > 0 (sign of x kept).  On the device the float form is a truncated-quotient FMA, which is what the
+// reference's device build does (core/numerics/macros.hpp:41); both are exact for the |x| < 4 pi that occur here.
+template <class T>
+PHX_HD T fmod_t(T x, T y) {
+#if defined(__CUDA_ARCH__)
+  if constexpr (sizeof(T) == 4) {
+    return fmaf(-truncf(x * (1.0f / y)), y, x);
+  } else {
+    return fmod(x, y);
+  }
+#else
+  return std::fmod(x, y);
+#endif
+}
+
+template <class T>
+PHX_HD T sq(T x) {
+  return x * x;
+}
+
+// Precision-generic wrappers: float arguments go to the float routines on both host and device, double to double.
+#define PHX_MATH1(name)                             \
+  PHX_HD float name##_t(float x) { return std::name(x); } \
+  PHX_HD double name##_t(double x) { return std::name(x); }
+#if defined(__CUDA_ARCH__)
+#undef PHX_MATH1
+#define PHX_MATH1(name)                             \
+  PHX_HD float name##_t(float x) { return name##f(x); } \
+  PHX_HD double name##_t(double x) { return name(x); }
+#endif
+PHX_MATH1(exp)
+PHX_MATH1(log)
+PHX_MATH1(sqrt)
+PHX_MATH1(cbrt)
+PHX_MATH1(expm1)
+PHX_MATH1(tanh)
+PHX_MATH1(acos)
+PHX_MATH1(cos)
+PHX_MATH1(sin)
+PHX_MATH1(fabs)
+PHX_MATH1(floor)
+PHX_MATH1(sinh)
+PHX_MATH1(log1p)
+#undef PHX_MATH1
+
+}  // namespace phx

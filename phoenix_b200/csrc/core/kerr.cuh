@@ -1,0 +1,202 @@
+// Kerr spacetime in modified Kerr-Schild coordinates of the BHAC flavour (MKS-BHAC):
+//   x0 = t,  x1 = ln r,  x2 with theta = x2 + (h/2) sin(2 x2),  x3 = phi.
+// The reference renderer evaluates the same metric (core/geometry/metric.hpp:26-221) and the geodesic equation in a
+// closed-form Christoffel contraction (core/geometry/geodesic.hpp:81-195).  Here the metric is kept as its seven
+// non-zero covariant components and six non-zero contravariant ones, and the geodesic right-hand side is formed from
+// the analytic first derivatives d g_{mu nu} / d x1 and d g_{mu nu} / d x2 (the metric depends on x1, x2 only):
+//   Gamma^mu(U, V) = g^{mu nu} a_nu,
+//   a_nu = 1/2 [ (U^1 D1 + U^2 D2)_{nu b} V^b + (V^1 D1 + V^2 D2)_{nu b} U^b - delta_{nu 1} U.D1.V - delta_{nu 2} U.D2.V ]
+// which is the textbook Gamma_{nu ab} = (d_a g_{nu b} + d_b g_{nu a} - d_nu g_{ab}) / 2 with the vanishing t- and
+// phi-derivatives dropped.  Everything lives in registers: ~60 flops of geometry and ~110 FMAs of contraction for the
+// two accelerations (k.k and k.F) an RK4 stage needs.
+#pragma once
+
+#include "defs.cuh"
+
+namespace phx {
+
+// Geometry of one point: everything the metric, its inverse and its derivatives share.
+template <class T>
+struct KerrPt {
+  T r;    // exp(x1)
+  T s;    // sin(theta)
+  T c;    // cos(theta)
+  T s2;   // sin^2(theta)
+  T tp;   // d theta / d x2
+  T tpp;  // d^2 theta / d x2^2
+  T sig;  // Sigma = r^2 + a^2 cos^2(theta)
+  T q;    // 2 r / Sigma
+};
+
+// Non-zero covariant components g_{mu nu} (symmetric).
+template <class T>
+struct Cov {
+  T tt, t1, t3, x11, x13, x22, x33;
+};
+
+// Non-zero contravariant components g^{mu nu} (symmetric; g^{t3} = g^{t2} = 0).
+template <class T>
+struct Contra {
+  T tt, t1, x11, x13, x22, x33;
+};
+
+template <class T>
+PHX_HD KerrPt<T> kerr_point(T a, T hs, T x1, T x2) {
+  KerrPt<T> p;
+  p.r = exp_t(x1);
+  T s2x, c2x;
+  sincos_t(T(2) * x2, &s2x, &c2x);
+  const T th = x2 + T(0.5) * hs * s2x;
+  p.tp = T(1) + hs * c2x;
+  p.tpp = T(-2) * hs * s2x;
+  sincos_t(th, &p.s, &p.c);
+  p.s2 = p.s * p.s;
+  p.sig = p.r * p.r + a * a * p.c * p.c;
+  p.q = T(2) * p.r / p.sig;
+  return p;
+}
+
+template <class T>
+PHX_HD Cov<T> cov_metric(const KerrPt<T>& p, T a) {
+  Cov<T> g;
+  const T opq = T(1) + p.q;
+  g.tt = p.q - T(1);
+  g.t1 = p.q * p.r;
+  g.t3 = -a * p.s2 * p.q;
+  g.x11 = opq * p.r * p.r;
+  g.x13 = -a * p.s2 * opq * p.r;
+  g.x22 = p.sig * p.tp * p.tp;
+  g.x33 = p.s2 * (p.sig + a * a * p.s2 * opq);
+  return g;
+}
+
+template <class T>
+PHX_HD Contra<T> contra_metric(const KerrPt<T>& p, T a) {
+  Contra<T> u;
+  const T isig = T(1) / p.sig;
+  const T ir = T(1) / p.r;
+  u.tt = -(T(1) + p.q);
+  u.t1 = T(2) * isig;
+  u.x11 = isig * ((p.r - T(2)) * p.r + a * a) * ir * ir;
+  u.x13 = a * isig * ir;
+  u.x22 = isig / (p.tp * p.tp);
+  u.x33 = isig / p.s2;
+  return u;
+}
+
+// g_{mu nu} U^mu V^nu
+template <class T>
+PHX_HD T dot(const Cov<T>& g, const T U[4], const T V[4]) {
+  return g.tt * U[0] * V[0] + g.t1 * (U[0] * V[1] + U[1] * V[0]) + g.t3 * (U[0] * V[3] + U[3] * V[0]) +
+         g.x11 * U[1] * V[1] + g.x13 * (U[1] * V[3] + U[3] * V[1]) + g.x22 * U[2] * V[2] + g.x33 * U[3] * V[3];
+}
+
+// out = M V for a symmetric matrix with the metric's sparsity pattern (works for Cov and the derivative sets).
+template <class T, class M>
+PHX_HD void symv(const M& m, const T V[4], T out[4]) {
+  out[0] = m.tt * V[0] + m.t1 * V[1] + m.t3 * V[3];
+  out[1] = m.t1 * V[0] + m.x11 * V[1] + m.x13 * V[3];
+  out[2] = m.x22 * V[2];
+  out[3] = m.t3 * V[0] + m.x13 * V[1] + m.x33 * V[3];
+}
+
+template <class T>
+PHX_HD void raise(const Contra<T>& u, const T Vd[4], T out[4]) {
+  out[0] = u.tt * Vd[0] + u.t1 * Vd[1];
+  out[1] = u.t1 * Vd[0] + u.x11 * Vd[1] + u.x13 * Vd[3];
+  out[2] = u.x22 * Vd[2];
+  out[3] = u.x13 * Vd[1] + u.x33 * Vd[3];
+}
+
+// Full 4x4 covariant metric (host-side tools and the decode path; the render path uses Cov directly).
+template <class T>
+PHX_HD void metric_dd_full(T a, T hs, T x1, T x2, T g[4][4]) {
+  const KerrPt<T> p = kerr_point(a, hs, x1, x2);
+  const Cov<T> c = cov_metric(p, a);
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++) g[i][j] = T(0);
+  g[0][0] = c.tt;
+  g[0][1] = g[1][0] = c.t1;
+  g[0][3] = g[3][0] = c.t3;
+  g[1][1] = c.x11;
+  g[1][3] = g[3][1] = c.x13;
+  g[2][2] = c.x22;
+  g[3][3] = c.x33;
+}
+
+template <class T>
+PHX_HD void metric_uu_full(T a, T hs, T x1, T x2, T g[4][4]) {
+  const KerrPt<T> p = kerr_point(a, hs, x1, x2);
+  const Contra<T> c = contra_metric(p, a);
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++) g[i][j] = T(0);
+  g[0][0] = c.tt;
+  g[0][1] = g[1][0] = c.t1;
+  g[1][1] = c.x11;
+  g[1][3] = g[3][1] = c.x13;
+  g[2][2] = c.x22;
+  g[3][3] = c.x33;
+}
+
+// First derivatives of the covariant metric with respect to x1 (D1) and x2 (D2).
+template <class T>
+PHX_HD void cov_derivs(const KerrPt<T>& p, T a, Cov<T>* D1, Cov<T>* D2) {
+  const T a2 = a * a, r = p.r, r2 = r * r, q = p.q, opq = T(1) + q;
+  // x1: dr/dx1 = r, dSigma/dx1 = 2 r^2, dq/dx1 = q (1 - 2 r^2 / Sigma)
+  const T q1 = q * (T(1) - T(2) * r2 / p.sig);
+  D1->tt = q1;
+  D1->t1 = (q1 + q) * r;
+  D1->t3 = -a * p.s2 * q1;
+  D1->x11 = (q1 + T(2) * opq) * r2;
+  D1->x13 = -a * p.s2 * (q1 + opq) * r;
+  D1->x22 = T(2) * r2 * p.tp * p.tp;
+  D1->x33 = p.s2 * (T(2) * r2 + a2 * p.s2 * q1);
+  // x2: d(sin^2)/dx2 = 2 s c theta', dSigma/dx2 = -2 a^2 s c theta', dq/dx2 = -q dSigma / Sigma
+  const T sc2 = T(2) * p.s * p.c * p.tp;
+  const T sig2 = -a2 * sc2;
+  const T q2 = -q * sig2 / p.sig;
+  D2->tt = q2;
+  D2->t1 = q2 * r;
+  D2->t3 = -a * (sc2 * q + p.s2 * q2);
+  D2->x11 = q2 * r2;
+  D2->x13 = -a * r * (sc2 * opq + p.s2 * q2);
+  D2->x22 = sig2 * p.tp * p.tp + T(2) * p.sig * p.tp * p.tpp;
+  D2->x33 = sc2 * (p.sig + a2 * p.s2 * opq) + p.s2 * (sig2 + a2 * (sc2 * opq + p.s2 * q2));
+}
+
+// Right-hand side of the geodesic equation and of the parallel transport of a polarization vector F:
+//   dk^mu/dl = -Gamma^mu_ab k^a k^b,   dF^mu/dl = -Gamma^mu_ab k^a F^b.
+template <class T>
+PHX_HD void geodesic_accel(T a, T hs, T x1, T x2, const T k[4], const T F[4], T dk[4], T dF[4]) {
+  const KerrPt<T> p = kerr_point(a, hs, x1, x2);
+  Cov<T> D1, D2;
+  cov_derivs(p, a, &D1, &D2);
+  const Contra<T> u = contra_metric(p, a);
+  T Pk[4], Qk[4], PF[4], QF[4];
+  symv(D1, k, Pk);  // D1 k
+  symv(D2, k, Qk);  // D2 k
+  symv(D1, F, PF);  // D1 F
+  symv(D2, F, QF);  // D2 F
+  const T kD1k = Pk[0] * k[0] + Pk[1] * k[1] + Pk[2] * k[2] + Pk[3] * k[3];
+  const T kD2k = Qk[0] * k[0] + Qk[1] * k[1] + Qk[2] * k[2] + Qk[3] * k[3];
+  const T kD1F = Pk[0] * F[0] + Pk[1] * F[1] + Pk[2] * F[2] + Pk[3] * F[3];
+  const T kD2F = Qk[0] * F[0] + Qk[1] * F[1] + Qk[2] * F[2] + Qk[3] * F[3];
+  T ak[4], aF[4];
+  for (int n = 0; n < 4; n++) {
+    ak[n] = k[1] * Pk[n] + k[2] * Qk[n];
+    aF[n] = T(0.5) * (k[1] * PF[n] + k[2] * QF[n] + F[1] * Pk[n] + F[2] * Qk[n]);
+  }
+  ak[1] -= T(0.5) * kD1k;
+  ak[2] -= T(0.5) * kD2k;
+  aF[1] -= T(0.5) * kD1F;
+  aF[2] -= T(0.5) * kD2F;
+  T gk[4], gF[4];
+  raise(u, ak, gk);
+  raise(u, aF, gF);
+  for (int n = 0; n < 4; n++) {
+    dk[n] = -gk[n];
+    dF[n] = -gF[n];
+  }
+}
+
+}  // namespace phx
