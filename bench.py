@@ -1,0 +1,357 @@
+"""Benchmark of the PHOENIX-B200 raymarch path: ray-steps/s on the plain-GPU-path workload.
+
+Workload (one bench step = one pass of the hot path over one batch): a synthetic BHAC-format snapshot with a
+192x96x96 base grid in 8^3 blocks, base + 2 refinement levels (15.6M cells, 8 FP32 primitives per cell, 0.5 GB on the
+device), seed 0; three 512x512 images at inclinations 10, 60 and 163 deg, 230 GHz, m_unit 1.2e18, FoV 40 r_g, the
+reference's default integration settings.  Inputs are resident in HBM when the timed region starts; the snapshot
+(0.5 GB) is larger than L2 and L2 is also flushed (256 MB write) before every timed step.
+
+usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision fp32|fp64|mixed]
+Multi-GPU: one process per GPU under torch.distributed.run; every rank renders the same three images (weak scaling,
+no data-path collective); times are the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import hashlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+GEN = os.path.join(ROOT, "phoenix_b200", "_build", "phx_gen_snapshot")
+REF_CPU = os.path.join(ROOT, "oracle", "_ref", "ref_render_fp32")
+
+WORKLOAD = dict(base=(192, 96, 96), nlevels=3, refine=(3.5, 25.0, 0.55), seed=0, img=512,
+                inclinations=(10.0, 60.0, 163.0), frequency=230e9, m_unit=1.2e18)
+# Algorithmic FP32 flops per unit of work ("Roofline"): per ray-step, per plasma sample, per
+# (sample, frequency).
+FLOPS = dict(step=1800.0, sample=900.0, freq=850.0)
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def snapshot_files(w=WORKLOAD, root=None):
+    """Generate (once per machine) the workload's snapshot; returns (dump, grid)."""
+    key = hashlib.sha1(json.dumps([w["base"], w["nlevels"], w["refine"], w["seed"]]).encode()).hexdigest()[:12]
+    d = os.path.join(root or tempfile.gettempdir(), "phx_bench_" + key)
+    dump, grid = os.path.join(d, "dump.dat"), os.path.join(d, "grid.in")
+    done = os.path.join(d, "done")
+    if not os.path.exists(done):
+        os.makedirs(d, exist_ok=True)
+        args = [GEN, "--out", d, "--seed", str(w["seed"]), "--base", *map(str, w["base"]), "--nlevels",
+                str(w["nlevels"]), "--nws", "0", "--refine", *map(str, w["refine"])]
+        subprocess.check_call(args, stdout=subprocess.DEVNULL)
+        open(done, "w").close()
+    return dump, grid
+
+
+def render_kwargs(w=WORKLOAD):
+    return dict(img=w["img"], frequencies=[w["frequency"]], m_unit=w["m_unit"])
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc or not self.path:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 7:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def _cpu_passes(dump, grid, w, stride, ncores, repeat, tmp):
+    """Time `repeat` passes of the CPU path over a strided pixel sample of the workload's three images (snapshot read
+    once).  Returns (kind, pixels per pass, [(steps, seconds) per pass])."""
+    pix = np.arange(0, w["img"] * w["img"], stride, dtype=np.int64)
+    pix = ((pix + (pix // w["img"]) * 7) % (w["img"] * w["img"])).astype(np.int32)
+    if os.path.exists(REF_CPU):
+        from tests.golden.cases import write_config
+        case = dict(snapshot="cfg1", inclination=w["inclinations"][0], img_width=w["img"], img_height=w["img"],
+                    frequencies=[w["frequency"]], m_unit=w["m_unit"])
+        cfg = os.path.join(tmp, "c.toml")
+        write_config(cfg, case, dump, grid, tmp)
+        with open(cfg) as f:
+            text = f.read().replace("nlevels = 3", f"nlevels = {w['nlevels']}")
+        with open(cfg, "w") as f:
+            f.write(text)
+        pfile = os.path.join(tmp, "pix.bin")
+        pix.tofile(pfile)
+        out = subprocess.check_output([REF_CPU, cfg, "--pixels", pfile, "--threads", str(ncores), "--inclinations",
+                                       ",".join(str(i) for i in w["inclinations"]), "--repeat", str(repeat)])
+        passes = [json.loads(l) for l in out.decode().splitlines() if l.strip()]
+        return "reference", pix.size * len(w["inclinations"]), [(p["steps"], p["seconds"]) for p in passes]
+    from oracle.oracle import Oracle
+    os_ = [Oracle(dump, grid, inclination=i, img_width=w["img"], img_height=w["img"], frequencies=(w["frequency"],),
+                  m_unit=w["m_unit"], nlevels=w["nlevels"]) for i in w["inclinations"]]
+    passes = []
+    for _ in range(repeat):
+        st_sum, sec = 0, 0.0
+        for o in os_:
+            _, st, secs = o.render(pix, threads=ncores)
+            st_sum += int(st[:, 0].sum())
+            sec += secs
+        passes.append((st_sum, sec))
+    for o in os_:
+        o.close()
+    return "port", pix.size * len(w["inclinations"]), passes
+
+
+def cpu_stride(dump, grid, w, ncores, tmp, seconds_target=10.0):
+    """Pixel stride that makes one pass over the three images take about `seconds_target`."""
+    _, _, passes = _cpu_passes(dump, grid, w, 1024, ncores, 1, tmp)
+    return int(np.clip(1024 * passes[0][1] / seconds_target, 1, 1024))
+
+
+def cpu_baseline(dump, grid, w, threads=0, repeat=1, stride=None):
+    """The reference's own CPU path (its FP32 build, OpenMP over all host threads) -- or the FP64 C oracle port when
+    the reference could not be compiled -- on a strided pixel sample of the workload's three images, sized by a short
+    calibration run to about 10 s of pixel-loop wall time per pass.
+    Returns (ray-steps/s per pass list, cores, kind, description)."""
+    ncores = threads or os.cpu_count()
+    with tempfile.TemporaryDirectory() as tmp:
+        stride = stride or cpu_stride(dump, grid, w, ncores, tmp)
+        kind, npix, passes = _cpu_passes(dump, grid, w, stride, ncores, repeat, tmp)
+    desc = (f"{npix} rays per pass (every {stride}th pixel of each {w['img']}^2 image, 3 inclinations), "
+            f"{'reference FP32 CPU build (oracle/_ref)' if kind == 'reference' else 'FP64 C oracle port'}, "
+            f"{ncores} OpenMP threads, pixel-loop wall time")
+    return [st / sec for st, sec in passes], ncores, kind, desc, passes
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    dump, grid = snapshot_files()
+    K = max(1, args.steps)
+    rates, cores, kind, desc, passes = cpu_baseline(dump, grid, WORKLOAD, repeat=args.warmup + K)
+    timed = passes[args.warmup:]
+    steps = sum(p[0] for p in timed)
+    secs = sum(p[1] for p in timed)
+    value = steps / secs
+    line = {"metric": "ray-steps/s", "value": value, "unit": "ray-steps/s", "n_gpus": args.gpus, "steps": K,
+            "warmup": args.warmup, "ms_per_step": 1e3 * secs / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": {"workload": "plain GPU path: 192x96x96 base grid, 8^3 blocks, 3 AMR levels (15.6M cells), "
+                                   "3 x 512^2 images at 10/60/163 deg, 230 GHz, m_unit 1.2e18",
+                       "sample": desc},
+            "cpu_baseline": {"value": value, "unit": "ray-steps/s", "cores": cores, "kind": kind, "sample": desc},
+            "e2e": {"value": value, "unit": "ray-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64", "mixed"])
+    ap.add_argument("--img", type=int, default=WORKLOAD["img"], help="image side (profiling runs use smaller)")
+    ap.add_argument("--period", type=int, default=0)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+
+    import phoenix_b200 as P
+
+    rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+    w = dict(WORKLOAD)
+    w["img"] = args.img
+
+    if rank == 0:
+        dump, grid = snapshot_files(w)
+    if world > 1:
+        dist.barrier()
+    dump, grid = snapshot_files(w)
+    t0 = time.time()
+    snap = P.Snapshot.load(dump, grid, nlevels=w["nlevels"])
+    log(f"[rank {rank}] snapshot resident: {snap.nbytes() / 1e9:.3f} GB in {time.time() - t0:.1f} s")
+
+    stream = torch.cuda.Stream(device=dev)
+    params = [P.make_params(inclination=i, precision=args.precision, period=args.period, **render_kwargs(w))
+              for i in w["inclinations"]]
+    npix = w["img"] * w["img"]
+    jobs = torch.from_numpy(P.schedule_morton(w["img"], w["img"])).to(dev)
+    res = [torch.zeros((npix, 1, 6), dtype=torch.float64, device=dev) for _ in params]
+    ctr = torch.zeros((len(params), P.NUM_COUNTERS), dtype=torch.int64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def one_step():
+        ctr.zero_()
+        for k, p in enumerate(params):
+            snap.render_async(p, jobs.data_ptr(), npix, res[k].data_ptr(), ctr[k].data_ptr(), 0, stream.cuda_stream)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            one_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    kev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in params]
+           for _ in range(args.steps)]
+    steps_total = 0
+    nplasma_total = 0
+    with ClockSampler(local) as clk:
+        for s in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(s & 0xFF)  # L2 flush, outside the timed region
+                ev[s][0].record(stream)
+                ctr.zero_()
+                for k, p in enumerate(params):
+                    kev[s][k][0].record(stream)
+                    snap.render_async(p, jobs.data_ptr(), npix, res[k].data_ptr(), ctr[k].data_ptr(), 0,
+                                      stream.cuda_stream)
+                    kev[s][k][1].record(stream)
+                ev[s][1].record(stream)
+            stream.synchronize()
+            c = ctr.cpu().numpy()
+            steps_total += int(c[:, P.CTR["steps"]].sum())
+            nplasma_total += int(c[:, P.CTR["nplasma"]].sum())
+        torch.cuda.synchronize()
+    clocks = clk.summary()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    kms = [a.elapsed_time(b) for row in kev for a, b in row]
+    t_local = torch.tensor([ms], dtype=torch.float64, device=dev)
+    n_local = torch.tensor([steps_total], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t_local, op=dist.ReduceOp.MAX)
+        dist.all_reduce(n_local, op=dist.ReduceOp.SUM)
+    ms_max = float(t_local.item())
+    value = float(n_local.item()) / (ms_max * 1e-3)
+
+    # end to end through the public API: pinned host job list in, host FreqOut image out, every step
+    e2e = None
+    if not args.no_e2e:
+        jobs_h = torch.from_numpy(P.schedule_morton(w["img"], w["img"])).pin_memory()
+        outs = [torch.zeros((w["img"], w["img"], 1, 6), dtype=torch.float64).pin_memory() for _ in params]
+        for k, p in enumerate(params):
+            snap.render(p, jobs=jobs_h.numpy(), out=outs[k].numpy())
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        e_steps = 0
+        t1 = time.perf_counter()
+        for _ in range(args.steps):
+            for k, p in enumerate(params):
+                _, info = snap.render(p, jobs=jobs_h.numpy(), out=outs[k].numpy())
+                e_steps += info["steps"]
+        e_s = time.perf_counter() - t1
+        te = torch.tensor([e_s], dtype=torch.float64, device=dev)
+        ne = torch.tensor([e_steps], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+            dist.all_reduce(ne, op=dist.ReduceOp.SUM)
+        e2e = {"value": float(ne.item()) / float(te.item()), "unit": "ray-steps/s",
+               "h2d_bytes_per_step": len(params) * npix * 4,
+               "d2h_bytes_per_step": len(params) * (npix * 48 + P.NUM_COUNTERS * 8)}
+
+    if rank == 0:
+        nimg = len(params) * args.steps
+        nfreq = 1
+        flops = FLOPS["step"] * steps_total + (FLOPS["sample"] + nfreq * FLOPS["freq"]) * nplasma_total
+        kavg = sum(kms) / len(kms)
+        achieved = flops / len(kms) / (kavg * 1e-3) / 1e12
+        props = torch.cuda.get_device_properties(dev)
+        peak = props.multi_processor_count * 128 * 2 * 1.965e9 / 1e12
+        line = {
+            "metric": "ray-steps/s", "value": value, "unit": "ray-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else args.precision,
+            "data": "synthetic",
+            "config": {"workload": "plain GPU path: 192x96x96 base grid, 8^3 blocks, 3 AMR levels (15.6M cells, FP32 "
+                                   f"primitives), 3 x {w['img']}^2 images at 10/60/163 deg, 230 GHz, m_unit 1.2e18",
+                       "precision": args.precision, "images_per_step": len(params), "rays_per_step": len(params) * npix,
+                       "l2": "flushed (256 MB write) before every timed step; snapshot 0.5 GB > L2",
+                       "parallelism": f"{world} GPU(s), independent replicas"},
+            "images_per_s": nimg / (ms_max * 1e-3) * world,
+            "rays_per_s": nimg * npix / (ms_max * 1e-3) * world,
+            "ray_steps_per_step": steps_total / args.steps,
+            "gpu_launches": len(kms),
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "note": "FP32-issue roofline: algorithmic flops per launch (per-step/sample/frequency "
+                                 "constants) over the average launch time; peak = SMs x 128 lanes x 2 x 1965 MHz "
+                                 "(nominal; no measured FP32 peak exists for this pool)"},
+            "clocks": clocks,
+            "e2e": e2e,
+        }
+        if world == 1 and not args.no_cpu:
+            rates, cores, kind, desc, _ = cpu_baseline(dump, grid, w)
+            line["cpu_baseline"] = {"value": rates[0], "unit": "ray-steps/s", "cores": cores, "kind": kind,
+                                    "sample": desc}
+        print(json.dumps(line), flush=True)
+    snap.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,166 @@
+/* PHOENIX-B200: C ABI of the B200-native raymarch path of the PHOENIX GRRT renderer.
+ *
+ * The path: for each pixel, a null geodesic is marched from a distant camera towards a Kerr black hole with RK4 in
+ * MKS-BHAC coordinates; at each step the block-AMR BHAC GRMHD snapshot is sampled and the polarized (I, Q, U, V)
+ * thermal-synchrotron transfer operator is folded into the pixel's accumulator.  It replaces the reference's
+ * device::render (nohgz/phoenix src/device/kernel.cuh:57-66, src/device/kernel.cu:284-360) and, for the CPU build,
+ * host::jobs::process (src/host/render/jobs.hpp:50-92), both of which call core::pixel::render_pixel
+ * (src/core/render/pixel.hpp:134-224) once per pixel.
+ *
+ * Conventions: every call returns 0 on success or a negative PHX_E* code, and phx_last_error() (per host thread)
+ * describes the failure; nothing throws across this boundary.  Sizes are in elements unless stated.  Snapshots are
+ * device-resident until destroyed.  One render at a time per snapshot handle and stream from one host thread.
+ */
+#ifndef PHOENIX_B200_H
+#define PHOENIX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PHX_MAX_FREQS 32
+#define PHX_MAX_LEVELS 16
+
+enum {
+  PHX_OK = 0,
+  PHX_E_INVALID = -1,  /* bad argument (null pointer, size out of range, inconsistent tables) */
+  PHX_E_IO = -2,       /* dump / grid file missing, short or malformed */
+  PHX_E_CUDA = -3,     /* CUDA runtime error (no device, out of memory, launch failure) */
+  PHX_E_TIMEOUT = -4,  /* a device wait ran out of iterations; the kernel returned early */
+  PHX_E_UNSUPPORTED = -5
+};
+
+/* Arithmetic of a render. */
+enum {
+  PHX_PREC_FP32 = 0,  /* FP32 throughout after the FP64 camera set-up */
+  PHX_PREC_FP64 = 1,  /* FP64 throughout */
+  PHX_PREC_MIXED = 2  /* FP32 bulk, FP64 near the horizon, in the null renormalisation, for large-depth segment
+                         operators, and Kahan-summed Stokes vectors */
+};
+
+/* Snapshot creation flags. */
+enum {
+  PHX_SNAP_F64_PRIMS = 1 /* also keep FP64 primitives on the device (FP64 renders then read them) */
+};
+
+/* One (pixel, frequency) result; binary-identical to the reference's core::pixel::FreqOut
+ * (src/core/render/pixel.hpp:26-29).  Stored at index (i * img_height + j) * nfreqs + f. */
+typedef struct {
+  double IQUV[4]; /* erg / s / cm^2 / Hz / sr (Jy / 1e23) */
+  double tau, tauF;
+} PhxFreqOut;
+
+/* A decoded snapshot in host memory (what host::bhac_io::load leaves in the reference's core::bhac::Model,
+ * src/core/model/bhac.hpp:131-173, src/host/io/bhac_io.hpp:331-499). */
+typedef struct {
+  int32_t nleafs;
+  int32_t nx[3];       /* cells per block */
+  int32_t ng[3];       /* base-level blocks per dimension */
+  int32_t nlevels;     /* levels of the leaf maps */
+  double a, hslope, gam;
+  double x_lo[3], x_hi[3];           /* domain in (x1 = ln r, x2, x3), radians */
+  const double* lb;                  /* [nleafs][3] block origins */
+  const double* dxc;                 /* [nleafs][3] cell sizes */
+  const float* prim_f32;             /* [nleafs][nx0*nx1*nx2][8] rho, u, u^1..3, B^1..3 (required) */
+  const double* prim_f64;            /* same in FP64, or NULL */
+  const int32_t* const* level_map;   /* nlevels maps, level L: [ng0<<L][ng1<<L][ng2<<L], leaf id or -1 */
+} PhxSnapshotDesc;
+
+/* Reader options (config.toml [grmhd] keys nspin, bpol, sfc, nlevels). */
+typedef struct {
+  int32_t nspin, bpol, sfc, nlevels;
+} PhxReadOptions;
+
+/* Everything a render reads besides the snapshot: the config.toml [camera], [black_hole], [integration] and
+ * [plasma] keys (src/host/io/config.hpp:300-370), plus the precision and launch knobs of this library. */
+typedef struct {
+  /* [camera] */
+  double inclination, fov_x, fov_y, r_cam, t_init, pa, phi;
+  int32_t img_width, img_height;
+  int32_t nfreqs;
+  double frequencies[PHX_MAX_FREQS];
+  /* [black_hole] */
+  double mass, distance;
+  /* [integration] */
+  double stepsize;
+  int32_t max_steps;
+  double horizon_margin;
+  int32_t max_order;
+  /* [plasma] */
+  double m_unit, r_low, r_high, beta_c, sigma_cut, thetae_min, thetae_max, rt_outer;
+  /* this library */
+  int32_t precision;   /* PHX_PREC_* */
+  double r_fp64;       /* mixed: FP64 RK4 inside r < r_fp64 * r_horizon (<= 0: default 1.5) */
+  double tau_fp64;     /* mixed: FP64 segment operator where h max|K| exceeds this (<= 0: default 0.1) */
+  int32_t block;       /* threads per block, 0 = default */
+  int32_t period;      /* march passes between lane refills, 0 = default */
+  int32_t blocks_per_sm; /* 0 = occupancy-derived */
+} PhxRenderParams;
+
+/* What a render reports (a superset of the reference's device::Info, src/device/kernel.cuh:23-30). */
+typedef struct {
+  char device[256];
+  int32_t sms, blocks, block, regs, local_bytes;
+  double upload_s, kernel_s;
+  int64_t steps, nplasma, bad;   /* sums over all rays */
+  int64_t scans;                 /* leaf lookups that fell back to the linear scan */
+  int64_t fp64_steps, fp64_ops;  /* mixed precision: RK4 steps and segment operators done in FP64 */
+} PhxRenderInfo;
+
+typedef struct PhxSnapshot PhxSnapshot;
+
+/* Fills p with the reference's default config.toml values (input/config.toml) and PHX_PREC_FP32. */
+void phx_default_params(PhxRenderParams* p);
+
+/* Uploads a decoded snapshot and keeps it resident (replaces upload_model, src/device/kernel.cu:265-280). */
+int phx_snapshot_create(const PhxSnapshotDesc* desc, int32_t flags, PhxSnapshot** out);
+
+/* Reads a BHAC dump + grid file, decodes it on the host and uploads it (host::bhac_io::load_bhac_grid + load,
+ * src/host/io/bhac_io.hpp:143-174, 331-499, then upload_model). */
+int phx_snapshot_load(const char* dump_file, const char* grid_file, const PhxReadOptions* opt, int32_t flags,
+                      PhxSnapshot** out);
+
+void phx_snapshot_destroy(PhxSnapshot* s);
+
+/* Host-only half of phx_snapshot_load: read and decode a BHAC dump into host memory (host::bhac_io::load with
+ * gpu_decode = false, src/host/io/bhac_io.hpp:331-499).  phx_bhac_describe fills a descriptor whose pointers refer
+ * into the host snapshot (valid until phx_bhac_free), ready for phx_snapshot_create on any device. */
+typedef struct PhxHostSnapshot PhxHostSnapshot;
+int phx_bhac_read(const char* dump_file, const char* grid_file, const PhxReadOptions* opt, int32_t flags,
+                  PhxHostSnapshot** out);
+int phx_bhac_describe(const PhxHostSnapshot* h, PhxSnapshotDesc* desc);
+void phx_bhac_free(PhxHostSnapshot* h);
+
+/* Device bytes held by a snapshot. */
+int64_t phx_snapshot_bytes(const PhxSnapshot* s);
+
+/* Pixel job list i * img_height + j, Morton-ordered (host::jobs::schedule with morton = true,
+ * src/host/render/jobs.hpp:18-45).  jobs holds img_width * img_height entries. */
+int phx_schedule_morton(int32_t img_width, int32_t img_height, int32_t* jobs);
+
+/* Renders the pixels `jobs` (host array, NULL = every pixel in Morton order) into the host array res
+ * (img_width * img_height * nfreqs records, index (i * img_height + j) * nfreqs + f; pixels not in jobs are left
+ * untouched).  Synchronous.  Replaces device::render (src/device/kernel.cu:284-360). */
+int phx_render(PhxSnapshot* s, const PhxRenderParams* p, const int32_t* jobs, int64_t njobs, PhxFreqOut* res,
+               PhxRenderInfo* info);
+
+/* Asynchronous form on a caller stream (cudaStream_t as void*, NULL = default stream) with device buffers:
+ * d_jobs (njobs pixel indices), d_res (img_width * img_height * nfreqs records), d_pixstats (NULL or
+ * 3 int32 per pixel: steps, nplasma, bad), d_counters (16 uint64, zeroed by the caller: queue head, steps, nplasma,
+ * bad, scans, fp64_steps, fp64_ops, ...).  Allocates nothing. */
+int phx_render_async(PhxSnapshot* s, const PhxRenderParams* p, const int32_t* d_jobs, int64_t njobs,
+                     PhxFreqOut* d_res, int32_t* d_pixstats, uint64_t* d_counters, void* stream);
+
+/* Description of the last error on this host thread. */
+const char* phx_last_error(void);
+
+/* Library version string. */
+const char* phx_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,126 @@
+"""PHOENIX-B200: the B200-native raymarch path of the PHOENIX GRRT renderer.
+
+Python front end of the C ABI (include/phoenix_b200.h).  A Snapshot is a BHAC block-AMR GRMHD snapshot resident on
+the GPU; Snapshot.render() marches every pixel's null geodesic through it and returns the reference's per-pixel
+FreqOut records (I, Q, U, V, tau, tauF) at index (i * img_height + j) * nfreqs + f, like the reference's
+device::render (src/device/kernel.cu:284-360).  The work runs in the sm_100a kernels of libphoenix_b200.so; there is
+no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import native
+from .native import (CTR, NUM_COUNTERS, PREC_FP32, PREC_FP64, PREC_MIXED, PhxError, PhxRenderInfo, make_params,
+                     schedule_morton)
+
+__all__ = ["Snapshot", "make_params", "schedule_morton", "flux", "pixel_solid_angle", "PhxError", "PREC_FP32",
+           "PREC_FP64", "PREC_MIXED", "CTR", "NUM_COUNTERS"]
+
+G_GRAV, M_SUN, C_LIGHT, KPC, JANSKY = 6.674e-8, 1.989e33, 2.99792458e10, 3.086e21, 1e23
+
+
+class Snapshot:
+    """A snapshot uploaded once and kept on the device until close()."""
+
+    def __init__(self, handle: int):
+        self._h = C.c_void_p(handle)
+
+    @classmethod
+    def load(cls, dump: str, grid: str, nspin: int = 3, bpol: int = 1, sfc: bool = True, nlevels: int = -1,
+             f64_prims: bool = False) -> "Snapshot":
+        """Read a BHAC dump + grid file (config.toml [grmhd] keys), decode it on the host and upload it."""
+        L = native.lib()
+        opt = native.PhxReadOptions(nspin, bpol, 1 if sfc else 0, nlevels)
+        h = C.c_void_p()
+        native.check(L.phx_snapshot_load(dump.encode(), grid.encode(), C.byref(opt),
+                                         native.SNAP_F64_PRIMS if f64_prims else 0, C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def from_arrays(cls, *, nx, ng, nlevels, a, hslope, gam, x_lo, x_hi, lb, dxc, prim_f32, level_maps,
+                    prim_f64=None) -> "Snapshot":
+        """Upload a decoded snapshot given as numpy arrays (lb, dxc: [nleafs, 3] float64; prim: [nleafs, cells, 8];
+        level_maps: nlevels int32 arrays)."""
+        L = native.lib()
+        lb = np.ascontiguousarray(lb, dtype=np.float64)
+        dxc = np.ascontiguousarray(dxc, dtype=np.float64)
+        pf = np.ascontiguousarray(prim_f32, dtype=np.float32)
+        pd = None if prim_f64 is None else np.ascontiguousarray(prim_f64, dtype=np.float64)
+        maps = [np.ascontiguousarray(m, dtype=np.int32) for m in level_maps]
+        ptrs = (C.c_void_p * len(maps))(*[m.ctypes.data for m in maps])
+        d = native.PhxSnapshotDesc()
+        d.nleafs = lb.shape[0]
+        d.nlevels = nlevels
+        for k in range(3):
+            d.nx[k], d.ng[k], d.x_lo[k], d.x_hi[k] = nx[k], ng[k], x_lo[k], x_hi[k]
+        d.a, d.hslope, d.gam = a, hslope, gam
+        d.lb, d.dxc, d.prim_f32 = lb.ctypes.data, dxc.ctypes.data, pf.ctypes.data
+        d.prim_f64 = pd.ctypes.data if pd is not None else None
+        d.level_map = C.cast(ptrs, C.c_void_p)
+        h = C.c_void_p()
+        native.check(L.phx_snapshot_create(C.byref(d), native.SNAP_F64_PRIMS if pd is not None else 0, C.byref(h)))
+        return cls(h.value)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def nbytes(self) -> int:
+        return native.lib().phx_snapshot_bytes(self._h)
+
+    def render(self, params=None, jobs=None, out=None, **kw):
+        """Render; returns (res[img_width, img_height, nfreqs, 6] float64, info dict).  `jobs`: pixel indices
+        i * img_height + j (default every pixel, Morton order); pixels outside `jobs` keep `out`'s values."""
+        p = params if params is not None else make_params(**kw)
+        W, H, F = p.img_width, p.img_height, p.nfreqs
+        res = out if out is not None else np.zeros((W, H, F, 6), dtype=np.float64)
+        if res.shape != (W, H, F, 6) or res.dtype != np.float64 or not res.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float64 array of shape (W, H, nfreqs, 6)")
+        info = PhxRenderInfo()
+        if jobs is None:
+            jp, nj = None, 0
+        else:
+            jobs = np.ascontiguousarray(jobs, dtype=np.int32)
+            jp, nj = jobs.ctypes.data, jobs.size
+        native.check(native.lib().phx_render(self._h, C.byref(p), jp, nj, res.ctypes.data, C.byref(info)))
+        return res, info.as_dict()
+
+    def render_async(self, params, d_jobs: int, njobs: int, d_res: int, d_counters: int, d_pixstats: int = 0,
+                     stream: int = 0):
+        """Launch on a CUDA stream with device pointers (e.g. torch tensors' data_ptr()); allocates nothing."""
+        native.check(native.lib().phx_render_async(self._h, C.byref(params), d_jobs or None, njobs, d_res,
+                                                   d_pixstats or None, d_counters, stream or None))
+
+    def close(self):
+        if self._h and self._h.value:
+            native.lib().phx_snapshot_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def pixel_solid_angle(p) -> float:
+    """Solid angle of one pixel [sr] (core/geometry/camera.hpp:28-32)."""
+    L = G_GRAV * p.mass * M_SUN / C_LIGHT / C_LIGHT
+    d = p.distance * KPC
+    return (p.fov_x / p.img_width * L / d) * (p.fov_y / p.img_height * L / d)
+
+
+def flux(res, params) -> np.ndarray:
+    """Total Stokes flux [Jy] per frequency (host/io/output.hpp:43-53): pixels with a non-finite I+Q+U+V skipped."""
+    r = res.reshape(-1, params.nfreqs, 6)[..., :4]
+    ok = np.isfinite(r.sum(axis=-1))
+    return np.where(ok[..., None], r, 0.0).sum(axis=0) * pixel_solid_angle(params) * JANSKY

@@ -83,6 +83,7 @@ PHX_HD T sq(T x) {
   PHX_HD double name##_t(double x) { return std::name(x); }
 #if defined(__CUDA_ARCH__)
 #undef PHX_MATH1
+
 #define PHX_MATH1(name)                             \
   PHX_HD float name##_t(float x) { return name##f(x); } \
   PHX_HD double name##_t(double x) { return name(x); }
@@ -101,5 +102,17 @@ PHX_MATH1(floor)
 PHX_MATH1(sinh)
 PHX_MATH1(log1p)
 #undef PHX_MATH1
+
+#if defined(__CUDA_ARCH__)
+PHX_HD float fmin_t(float x, float y) { return fminf(x, y); }
+PHX_HD double fmin_t(double x, double y) { return fmin(x, y); }
+PHX_HD float fmax_t(float x, float y) { return fmaxf(x, y); }
+PHX_HD double fmax_t(double x, double y) { return fmax(x, y); }
+#else
+PHX_HD float fmin_t(float x, float y) { return std::fmin(x, y); }
+PHX_HD double fmin_t(double x, double y) { return std::fmin(x, y); }
+PHX_HD float fmax_t(float x, float y) { return std::fmax(x, y); }
+PHX_HD double fmax_t(double x, double y) { return std::fmax(x, y); }
+#endif
 
 }  // namespace phx

@@ -1,0 +1,165 @@
+// Geodesic state and RK4 integrator of the raymarch.
+//
+// The state is (x^mu, k^mu, F^mu): position, wave vector and the parallel-transported camera polarization vector.
+// At FP32 it is carried as hi + lo float pairs updated by compensated (TwoSum) addition, and a ray in the southern
+// hemisphere is integrated in the mirror coordinate pi - x2 so that x2 keeps its precision next to the south pole
+// (the same device the reference's FP32 build uses, core/geometry/geodesic.hpp:200-256).  At FP64 the lo half is
+// unused.  The right-hand side is phx::geodesic_accel (kerr.cuh).  The step-size rule is RAPTOR's, capped at a
+// quarter of the current AMR cell (geodesic.hpp:267-292).
+#pragma once
+
+#include "defs.cuh"
+#include "kerr.cuh"
+
+namespace phx {
+
+// Knuth TwoSum of hi + d folded into (hi, lo), then renormalised (fast two-sum).
+template <class R>
+PHX_HD void comp_add(R& hi, R& lo, R d) {
+  const R s = hi + d;
+  const R bb = s - hi;
+  const R err = (hi - (s - bb)) + (d - bb);
+  lo += err;
+  const R s2 = s + lo;
+  lo = lo - (s2 - s);
+  hi = s2;
+}
+
+template <class R>
+struct GeoState {
+  R hi[12];  // x[0..3], k[4..7], F[8..11]
+  R lo[12];  // compensation (FP32 only)
+};
+
+// Initial state from the FP64 camera photon and polarization vector.
+template <class R, bool kComp>
+PHX_HD void geo_init(GeoState<R>& g, const double ph[8], const double F[4]) {
+  for (int i = 0; i < 8; i++) g.hi[i] = R(ph[i]);
+  for (int i = 0; i < 4; i++) g.hi[8 + i] = R(F[i]);
+  for (int i = 0; i < 12; i++) g.lo[i] = R(0);
+  if (kComp) {
+    for (int i = 0; i < 8; i++) g.lo[i] = R(ph[i] - (double)g.hi[i]);
+    for (int i = 0; i < 4; i++) g.lo[8 + i] = R(F[i] - (double)g.hi[8 + i]);
+  }
+}
+
+template <class R, bool kComp>
+PHX_HD R geo_get(const GeoState<R>& g, int i) {
+  return kComp ? g.hi[i] + g.lo[i] : g.hi[i];
+}
+
+// x2 measured from the nearer pole where the integrator folds (FP32), else x2 itself.
+template <class R, bool kComp>
+PHX_HD R pole_x2(const GeoState<R>& g) {
+  if (kComp && g.hi[2] > R(kHalfPi)) {
+    const R pi_hi = R(kPi), pi_lo = R(kPi - (double)R(kPi));
+    return (pi_hi - g.hi[2]) + (pi_lo - g.lo[2]);
+  }
+  return g.hi[2] + (kComp ? g.lo[2] : R(0));
+}
+
+// One classical RK4 step of length dt.  Stage sums are kept as (d0 + d3) and (d1 + d2) so that the update
+// ((d0 + d3) + 2 (d1 + d2)) dt/6 needs two 12-vectors instead of four.
+template <class R, bool kComp>
+PHX_HD void rk4_step(R a, R hs, GeoState<R>& g, R dt) {
+  const R pi_hi = R(kPi), pi_lo = R(kPi - (double)R(kPi));
+  const bool south = kComp && g.hi[2] > R(kHalfPi);
+  R inc[12], s03[12], s12[12];
+#pragma unroll
+  for (int i = 0; i < 12; i++) inc[i] = R(0);
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    R y[12];
+#pragma unroll
+    for (int i = 0; i < 12; i++) y[i] = kComp ? g.hi[i] + (g.lo[i] + inc[i]) : g.hi[i] + inc[i];
+    if (south) {
+      y[2] = (pi_hi - g.hi[2]) + ((pi_lo - g.lo[2]) - inc[2]);
+      y[6] = -y[6];
+      y[10] = -y[10];
+    }
+    R d[12];
+    d[0] = y[4];
+    d[1] = y[5];
+    d[2] = y[6];
+    d[3] = y[7];
+    geodesic_accel(a, hs, y[1], y[2], y + 4, y + 8, d + 4, d + 8);
+    if (south) {
+      d[2] = -d[2];
+      d[6] = -d[6];
+      d[10] = -d[10];
+    }
+#pragma unroll
+    for (int i = 0; i < 12; i++) {
+      if (q == 0) s03[i] = d[i];
+      if (q == 1) s12[i] = d[i];
+      if (q == 2) s12[i] += d[i];
+      if (q == 3) s03[i] += d[i];
+    }
+    if (q < 3) {
+      const R wdt = (q == 2 ? R(1) : R(0.5)) * dt;
+#pragma unroll
+      for (int i = 0; i < 12; i++) inc[i] = wdt * d[i];
+    }
+  }
+  const R dt6 = dt / R(6);
+#pragma unroll
+  for (int i = 0; i < 12; i++) {
+    const R du = (s03[i] + R(2) * s12[i]) * dt6;
+    if (kComp) {
+      comp_add(g.hi[i], g.lo[i], du);
+    } else {
+      g.hi[i] += du;
+    }
+  }
+}
+
+// FP64 RK4 step of an FP32 compensated state: the pair is widened to double, stepped, and split back.
+PHX_HD void rk4_step_widened(double a, double hs, GeoState<float>& g, double dt) {
+  GeoState<double> w;
+#pragma unroll
+  for (int i = 0; i < 12; i++) {
+    w.hi[i] = (double)g.hi[i] + (double)g.lo[i];
+    w.lo[i] = 0.0;
+  }
+  rk4_step<double, false>(a, hs, w, dt);
+#pragma unroll
+  for (int i = 0; i < 12; i++) {
+    g.hi[i] = (float)w.hi[i];
+    g.lo[i] = (float)(w.hi[i] - (double)g.hi[i]);
+  }
+}
+
+// RAPTOR step size (negative: the ray runs backwards from the camera), capped by a quarter of the AMR cell.
+// dxc == nullptr means no cap.
+template <class R>
+PHX_HD R step_size(R stepsize, R x2, const R k[4], const R* dxc, R tiny, R big) {
+  const R dlx1 = stepsize / (fabs_t(k[1]) + tiny);
+  const R dlx2 = stepsize * fmin_t(x2, R(kPi) - x2) / (fabs_t(k[2]) + tiny);
+  const R dlx3 = stepsize / (fabs_t(k[3]) + tiny);
+  const R i1 = R(1) / (fabs_t(dlx1) + tiny);
+  const R i2 = R(1) / (fabs_t(dlx2) + tiny);
+  const R i3 = R(1) / (fabs_t(dlx3) + tiny);
+  R grid = big;
+  if (dxc) {
+    const R s1 = dxc[0] / (fabs_t(k[1]) + tiny);
+    const R s2 = dxc[1] / (fabs_t(k[2]) + tiny);
+    const R s3 = dxc[2] / (fabs_t(k[3]) + tiny);
+    const R is1 = R(1) / (fabs_t(s1) + tiny);
+    const R is2 = R(1) / (fabs_t(s2) + tiny);
+    const R is3 = R(1) / (fabs_t(s3) + tiny);
+    grid = R(1) / (is1 + is2 + is3) / R(4);
+  }
+  return -fmin_t(R(1) / (i1 + i2 + i3), grid);
+}
+
+// Re-solve k^t from the spatial components so that g_{mu nu} k^mu k^nu = 0 (the larger root), as the reference
+// does for each plasma sample (geodesic.hpp:297-306, called from core/render/pixel.hpp:69-71).
+template <class R>
+PHX_HD void normalize_null(const Cov<R>& g, R k[4]) {
+  const R aa = g.tt;
+  const R beta = -(g.t1 * k[1] + g.t3 * k[3]) / aa;
+  const R gam = -(g.x11 * k[1] * k[1] + R(2) * g.x13 * k[1] * k[3] + g.x22 * k[2] * k[2] + g.x33 * k[3] * k[3]) / aa;
+  k[0] = beta + sqrt_t(beta * beta + gam);
+}
+
+}  // namespace phx

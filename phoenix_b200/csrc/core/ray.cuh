@@ -1,0 +1,277 @@
+// One ray of the raymarch as a resumable state machine.
+//
+// Ray::advance() performs exactly one pass of the reference's per-pixel loop (core/render/pixel.hpp:179-211):
+//   view the state -> liveness test -> process the PREVIOUS sample with the sampler cache seeded by this sample's
+//   leaf -> theta turning points -> grid-capped step size -> RK4 step.
+// Because the state is explicit, a warp can retire a finished ray and start a new one in the same lane while its
+// neighbours keep marching (the kernel's lane refill), instead of idling until the warp's longest ray ends.
+//
+// Precision policies:
+//   FP32   float everywhere after the FP64 camera set-up; compensated (hi, lo) geodesic state with south-pole
+//          folding; deviation-form transfer operator.
+//   FP64   double everywhere.
+//   Mixed  FP32 bulk plus four FP64 islands: RK4 steps inside r < r_fp64 (default 1.5 r_horizon), the null-condition
+//          renormalisation of each sample's wave vector, the segment operator where h max|K| > tau_fp64 (large
+//          optical / Faraday depth per segment), and Kahan summation of the Stokes vector.
+#pragma once
+
+#include "camera.cuh"
+#include "defs.cuh"
+#include "geodesic.cuh"
+#include "kerr.cuh"
+#include "sampler.cuh"
+#include "synchro.cuh"
+#include "transfer.cuh"
+
+namespace phx {
+
+enum class Mode : int { kFP32 = 0, kFP64 = 1, kMixed = 2 };
+
+template <Mode M>
+struct Policy;
+template <>
+struct Policy<Mode::kFP32> {
+  using R = float;
+  static constexpr bool kComp = true, kMixed = false;
+};
+template <>
+struct Policy<Mode::kFP64> {
+  using R = double;
+  static constexpr bool kComp = false, kMixed = false;
+};
+template <>
+struct Policy<Mode::kMixed> {
+  using R = float;
+  static constexpr bool kComp = true, kMixed = true;
+};
+
+// Render-wide constants (one image: camera, integration, plasma and frequencies).
+template <class R>
+struct RenderConsts {
+  int32_t W, H, nfreqs, max_steps, max_order;
+  double fov_x, fov_y, cos_pa, sin_pa;
+  CameraSpec cam;
+  R stepsize, r_out, cut_in, rt_outer;
+  R step_tiny, step_big;
+  R r_fp64, tau_fp64;
+  PlasmaView<R> pv;
+  R freq[kMaxFreqs], hconst[kMaxFreqs], jscale[kMaxFreqs];
+};
+
+// Diagnostic counters a ray adds to.
+struct RayCounters {
+  uint32_t steps, nplasma, bad, scans, fp64_steps, fp64_ops;
+};
+
+template <Mode M, class PT, int NF>
+struct Ray {
+  using Pol = Policy<M>;
+  using R = typename Pol::R;
+  static constexpr bool kComp = Pol::kComp, kMixed = Pol::kMixed;
+
+  GeoState<R> geo;
+  R px[4], pk[4], pF[4], pdl;
+  bool pvalid, terminate;
+  int steps, turns, bsign, nplasma, bad;
+  R thdot_prev, dl_prev;
+  int32_t pix;
+  StokesAcc<R, kMixed> acc[NF];
+
+  PHX_HD void init(const SnapView<R, PT>& s, const RenderConsts<R>& rc, int32_t pixel) {
+    pix = pixel;
+    const int i = pixel / rc.H, j = pixel % rc.H;
+    double alpha, beta;
+    pixel_impact(i, j, rc.W, rc.H, rc.fov_x, rc.fov_y, rc.cos_pa, rc.sin_pa, &alpha, &beta);
+    double ph[8], F1[4];
+    camera_photon(rc.cam, alpha, beta, ph);
+    camera_pol<R>(s.a, s.hs, ph, F1);
+    geo_init<R, kComp>(geo, ph, F1);
+#pragma unroll
+    for (int f = 0; f < NF; f++) acc[f].reset();
+    pvalid = false;
+    terminate = false;
+    steps = turns = nplasma = bad = 0;
+    bsign = beta < 0.0 ? -1 : (beta > 0.0 ? 1 : 0);
+    thdot_prev = dl_prev = R(0);
+  }
+
+  // One pass of the march loop; false once the ray has ended (its pending sample has then been processed).
+  PHX_HD bool advance(const SnapView<R, PT>& s, const RenderConsts<R>& rc, RayCounters& ctr) {
+    R cx[4], ck[4], cF[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      cx[i] = geo_get<R, kComp>(geo, i);
+      ck[i] = geo_get<R, kComp>(geo, 4 + i);
+      cF[i] = geo_get<R, kComp>(geo, 8 + i);
+    }
+    const R r = exp_t(cx[1]);
+    const bool alive = r < rc.r_out && r > rc.cut_in && steps < rc.max_steps && !terminate;
+    const bool need_leaf = pvalid && alive;
+    const bool need_dxc = alive && r < rc.rt_outer;
+    int L = -1;
+    R xw[4] = {cx[0], cx[1], cx[2], cx[3]};
+    if (need_leaf || need_dxc) {
+      wrap_coords(xw);
+      bool scanned = false;
+      L = find_leaf(s, xw, &scanned);
+      ctr.scans += scanned;
+    }
+    if (pvalid) {
+      int right = -1;
+      if (need_leaf) right = (exp_t(xw[1]) < R(1) || outside_domain(s, xw)) ? -1 : L;
+      process_sample(s, rc, right, ctr);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      px[i] = cx[i];
+      pk[i] = ck[i];
+      pF[i] = cF[i];
+    }
+    pdl = dl_prev;
+    pvalid = steps >= 1;
+    if (!alive) return false;
+
+    if (thdot_prev * ck[2] < R(0) && steps > 2) turns++;
+    thdot_prev = ck[2];
+    if ((bsign < 0 && turns > rc.max_order) || (bsign > 0 && turns > rc.max_order + 1)) terminate = true;
+
+    R dxcv[3];
+    const bool cap = need_dxc && L >= 0;
+    if (cap) {
+#pragma unroll
+      for (int d = 0; d < 3; d++) dxcv[d] = ldg(s.dxc + 3 * L + d);
+    }
+    const R x2 = pole_x2<R, kComp>(geo);
+    const R dl = step_size(rc.stepsize, x2, ck, cap ? dxcv : (const R*)nullptr, rc.step_tiny, rc.step_big);
+    if constexpr (kMixed) {
+      if (r < rc.r_fp64) {
+        rk4_step_widened((double)s.a, (double)s.hs, geo, (double)dl);
+        ctr.fp64_steps++;
+      } else {
+        rk4_step<R, kComp>(s.a, s.hs, geo, dl);
+      }
+    } else {
+      rk4_step<R, kComp>(s.a, s.hs, geo, dl);
+    }
+    dl_prev = fabs_t(dl);
+    steps++;
+    return true;
+  }
+
+  // The plasma stage of the pending sample (the reference's process_sample, core/render/pixel.hpp:52-123).
+  PHX_HD void process_sample(const SnapView<R, PT>& s, const RenderConsts<R>& rc, int right, RayCounters& ctr) {
+    R k[4] = {pk[0], pk[1], pk[2], pk[3]};
+    const R r = exp_t(px[1]);
+    {
+      const KerrPt<R> p0 = kerr_point(s.a, s.hs, px[1], px[2]);
+      const Cov<R> g0 = cov_metric(p0, s.a);
+      if (fabs_t(dot(g0, k, k)) > R(1e-6) && r > R(2)) {
+        if constexpr (kMixed) {
+          const KerrPt<double> pd = kerr_point((double)s.a, (double)s.hs, (double)px[1], (double)px[2]);
+          const Cov<double> gd = cov_metric(pd, (double)s.a);
+          double kd[4] = {k[0], k[1], k[2], k[3]};
+          normalize_null(gd, kd);
+          k[0] = R(kd[0]);
+        } else {
+          normalize_null(g0, k);
+        }
+      }
+    }
+    // sampler (sampler.hpp:387-427): wrap, domain, cached leaf or a fresh lookup of the re-wrapped point
+    R x[4] = {px[0], px[1], px[2], px[3]};
+    wrap_coords(x);
+    if (exp_t(x[1]) < R(1)) return;
+    if (outside_domain(s, x)) return;
+    int ig = right;
+    if (ig == -1 || !inside_cached(s, ig, x)) {
+      wrap_coords(x);
+      bool scanned = false;
+      ig = find_leaf(s, x, &scanned);
+      ctr.scans += scanned;
+    }
+    if (ig == -1) return;
+    R q[kNPrim];
+    interp_prims<R, PT, !kComp>(s, ig, x, q);
+    const KerrPt<R> p = kerr_point(s.a, s.hs, x[1], x[2]);
+    const Cov<R> g = cov_metric(p, s.a);
+    const Contra<R> u = contra_metric(p, s.a);
+    Fluid<R> fl;
+    if (!derive_fluid(rc.pv, s.gam, exp_t(x[1]), g, u, q, &fl)) return;
+    if (!(r < rc.rt_outer)) return;
+    // pitch angle of k to B in the plasma frame (tetrad.hpp:138-154)
+    const R Bn = sqrt_t(fabs_t(dot(g, fl.B, fl.B)));
+    const R kU = dot(g, k, fl.U);
+    R pitch;
+    if (Bn == R(0)) {
+      pitch = R(kHalfPi);
+    } else {
+      R mu = dot(g, k, fl.B) / (fabs_t(kU) * Bn);
+      if (fabs_t(mu) > R(1)) mu /= fabs_t(mu);
+      pitch = acos_t(mu);
+    }
+    if (pitch == R(0) || pitch == R(kPi)) return;
+    // polarization axes of the plasma frame with B as reference direction; EVPA rotation from the transported F1
+    R perp[4], para[4], omega;
+    observer_axes(g, sqrt_neg_g(p), k, fl.U, fl.B, perp, para, &omega);
+    const R C = dot(g, perp, pF), S = dot(g, para, pF);
+    const R nn = C * C + S * S;
+    const R c2 = (C * C - S * S) / nn, s2 = R(2) * C * S / nn;
+    const R ratio = -kU;  // nu_plasma / nu_camera
+    const SynchroSample<R> ss = synchro_sample(fl.theta_e, fl.n_e, fl.Bmag, pitch);
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+      if (f >= rc.nfreqs) break;
+      const R nu = rc.freq[f] * ratio;
+      const Coeffs<R> cf = synchro_coeffs(ss, nu, rc.jscale[f]);
+      R K[4][4], jv[4], E[4][4], Sg[4];
+      build_K(cf, c2, s2, K, jv);
+      const R h = pdl * rc.hconst[f];
+      bool fp64 = false;
+      if constexpr (kMixed) {
+        const R kmax = fmax_t(fmax_t(fabs_t(cf.aI), fabs_t(cf.rV)), fabs_t(cf.rQ));
+        fp64 = h * kmax > rc.tau_fp64;
+      }
+      if (fp64) {
+        double Kd[4][4], jd[4], Ed[4][4], Sd[4];
+        for (int a = 0; a < 4; a++) {
+          jd[a] = jv[a];
+          for (int b = 0; b < 4; b++) Kd[a][b] = K[a][b];
+        }
+        segment_operator<double>(Kd, jd, (double)h, Ed, Sd);
+        for (int a = 0; a < 4; a++) {
+          Sg[a] = R(Sd[a]);
+          for (int b = 0; b < 4; b++) E[a][b] = R(Ed[a][b]);
+        }
+        ctr.fp64_ops++;
+      } else {
+        segment_operator<R>(K, jv, h, E, Sg);
+      }
+      if (!all_finite(E, Sg)) {
+        bad++;
+        continue;
+      }
+      acc[f].add(E, Sg);
+      acc[f].tau += cf.aI * h;
+      acc[f].tauF += fabs_t(cf.rV * h);
+    }
+    nplasma++;
+  }
+
+  // FreqOut records (I, Q, U, V, tau, tauF as doubles) of this pixel; zeros when no plasma segment was crossed.
+  PHX_HD void write(double* out, int nfreqs) const {
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+      if (f >= nfreqs) break;
+      double* o = out + ((size_t)pix * nfreqs + f) * 6;
+      const bool any = nplasma > 0;
+      o[0] = any ? (double)acc[f].S[0] : 0.0;
+      o[1] = any ? (double)acc[f].S[1] : 0.0;
+      o[2] = any ? (double)acc[f].S[2] : 0.0;
+      o[3] = any ? (double)acc[f].S[3] : 0.0;
+      o[4] = any ? (double)acc[f].tau : 0.0;
+      o[5] = any ? (double)acc[f].tauF : 0.0;
+    }
+  }
+};
+
+}  // namespace phx

@@ -1,0 +1,240 @@
+// Block-AMR sampler: which leaf holds a point, and the plasma state there.
+//
+// Device layout of a snapshot (built once per snapshot, resident in HBM):
+//   lb, dxc   [nleafs][3]              block origin and cell size per leaf (in the render precision)
+//   prim      [nleafs][cells][8]       primitives per cell, 32 B per cell in FP32: a trilinear corner is two 128-bit
+//                                      loads, and the i / i+1 corners of a row share one 64-B segment
+//   fmap      [fd0][fd1][fd2] int32    leaf id per finest-level block slot: the per-level maps of the reference
+//                                      (core/model/sampler.hpp:55-82, host/io/bhac_io.hpp:257-309) flattened so that a
+//                                      lookup is one load instead of up to nlevels dependent loads; slot (i,j,k) holds
+//                                      the first leaf met walking levels coarse -> fine, exactly the map walk's answer.
+// Semantics follow the reference sampler (core/model/sampler.hpp:29-427): coordinate wrap with its -1e-6 shift of
+// x2, half-open leaf test with a +-1e-9 nudge away from the equator, inclusive cache test, linear-scan fallback,
+// block-local trilinear interpolation clamped at block faces, and the fluid derivation with the R_high/R_low
+// temperature prescription and emission cuts.
+#pragma once
+
+#include "defs.cuh"
+#include "kerr.cuh"
+
+namespace phx {
+
+template <class R, class PT>
+struct SnapView {
+  const R* lb;
+  const R* dxc;
+  const PT* prim;
+  const int32_t* fmap;
+  int32_t fd[3];
+  int32_t nleafs, nlevels, cells;
+  int32_t nx[3];
+  R x_lo[4], x_hi[4];
+  R w0[3];  // base-level block widths
+  R a, hs, gam;
+};
+
+// Per-render plasma constants.
+template <class R>
+struct PlasmaView {
+  R Ne, Bu, rhigh, rlow, ibc;
+  R sigma_cut, thetae_min, thetae_max, rt_outer;
+};
+
+template <class R>
+struct Fluid {
+  R U[4], B[4];
+  R n_e, Bmag, theta_e;
+};
+
+template <class R>
+PHX_HD void wrap_coords(R x[4]) {
+  const R TP = R(kTwoPi), PI = R(kPi);
+  x[3] = fmod_t(x[3], TP);
+  x[2] = fmod_t(x[2], PI) - R(1e-6);
+  if (x[3] < R(0)) x[3] = TP + x[3];
+  if (x[2] < R(0)) {
+    x[2] = -x[2];
+    x[3] = PI + x[3];
+  }
+}
+
+template <class R, class PT>
+PHX_HD bool outside_domain(const SnapView<R, PT>& s, const R x[4]) {
+  return x[1] > s.x_hi[1] || x[1] < s.x_lo[1] || x[2] < s.x_lo[2] || x[2] > s.x_hi[2] || x[3] < s.x_lo[3] ||
+         x[3] > s.x_hi[3];
+}
+
+template <class R>
+PHX_HD R leaf_nudge(const R x[4]) {
+  return x[2] > R(kHalfPi) ? R(-1e-9) : R(1e-9);
+}
+
+template <class R, class PT>
+PHX_HD int find_leaf_map(const SnapView<R, PT>& s, const R x[4], R small) {
+  const R up = R(1 << (s.nlevels - 1));
+  const R fi = (x[1] + small - s.x_lo[1]) / s.w0[0] * up;
+  const R fj = (x[2] + small - s.x_lo[2]) / s.w0[1] * up;
+  const R fk = (x[3] + small - s.x_lo[3]) / s.w0[2] * up;
+  if (fi < R(0) || fj < R(0) || fk < R(0)) return -1;
+  const int i = (int)fi, j = (int)fj, k = (int)fk;
+  if (i >= s.fd[0] || j >= s.fd[1] || k >= s.fd[2]) return -1;
+#if defined(__CUDA_ARCH__)
+  return __ldg(s.fmap + ((size_t)i * s.fd[1] + j) * s.fd[2] + k);
+#else
+  return s.fmap[((size_t)i * s.fd[1] + j) * s.fd[2] + k];
+#endif
+}
+
+template <class T>
+PHX_HD T ldg(const T* p) {
+#if defined(__CUDA_ARCH__)
+  return __ldg(p);
+#else
+  return *p;
+#endif
+}
+
+template <class R, class PT>
+PHX_HD bool inside_leaf(const SnapView<R, PT>& s, int leaf, const R x[4], R small) {
+  bool in = true;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const R lo = ldg(s.lb + 3 * leaf + d);
+    const R hi = lo + R(s.nx[d]) * ldg(s.dxc + 3 * leaf + d);
+    in = in && !(x[1 + d] + small < lo || x[1 + d] + small >= hi);
+  }
+  return in;
+}
+
+template <class R, class PT>
+PHX_HD bool inside_cached(const SnapView<R, PT>& s, int leaf, const R x[4]) {
+  bool in = true;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const R lo = ldg(s.lb + 3 * leaf + d);
+    const R hi = lo + R(s.nx[d]) * ldg(s.dxc + 3 * leaf + d);
+    in = in && !(x[1 + d] < lo || x[1 + d] > hi);
+  }
+  return in;
+}
+
+// Counts of the rare slow path, for diagnostics (incremented by the caller when `scanned` is set).
+template <class R, class PT>
+PHX_HD int find_leaf(const SnapView<R, PT>& s, const R x[4], bool* scanned) {
+  const R small = leaf_nudge(x);
+  const int cand = find_leaf_map(s, x, small);
+  if (cand >= 0 && inside_leaf(s, cand, x, small)) return cand;
+  const R eps = R(1e-6);
+  if (cand < 0 && (x[1] < s.x_lo[1] - eps || x[1] > s.x_hi[1] + eps || x[2] < s.x_lo[2] - eps ||
+                   x[2] > s.x_hi[2] + eps || x[3] < s.x_lo[3] - eps || x[3] > s.x_hi[3] + eps))
+    return -1;
+  // linear scan in leaf order: the first leaf whose half-open box holds the nudged point
+  *scanned = true;
+  for (int leaf = 0; leaf < s.nleafs; leaf++)
+    if (inside_leaf(s, leaf, x, small)) return leaf;
+  return -1;
+}
+
+// Trilinear interpolation of the 8 primitives inside one leaf, weights measured from the block's lower corner and
+// clamped at the block faces (no ghost cells).
+template <class R, class PT, bool kFloorBy1000>
+PHX_HD void interp_prims(const SnapView<R, PT>& s, int leaf, const R x[4], R q[kNPrim]) {
+  int c[3], ix[3];
+  R del[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const R lb = ldg(s.lb + 3 * leaf + d), dx = ldg(s.dxc + 3 * leaf + d);
+    const R u = (x[1 + d] - lb) / dx;
+    c[d] = (int)u;
+    if (c[d] >= s.nx[d]) c[d] = s.nx[d] - 1;
+    if (c[d] < 0) c[d] = 0;  // unreachable for finite points of the leaf; keeps every gather inside the block
+    ix[d] = kFloorBy1000 ? (int)(u + R(1000)) - 1000 : (int)floor_t(u);
+    del[d] = (ix[d] < 0) ? R(0) : (ix[d] > s.nx[d] - 2) ? R(1) : (x[1 + d] - (R(ix[d]) * dx + lb)) / dx;
+  }
+  const int nx0 = s.nx[0], nx01 = s.nx[0] * s.nx[1];
+  const int cip = c[0] + 1 < s.nx[0] ? c[0] + 1 : c[0];
+  const int cjp = c[1] + 1 < s.nx[1] ? c[1] + 1 : c[1];
+  const int ckp = c[2] + 1 < s.nx[2] ? c[2] + 1 : c[2];
+  const R b1 = R(1) - del[0], b2 = R(1) - del[1], b3 = R(1) - del[2];
+  const int ci[4] = {c[0], c[0], cip, cip};
+  const int cj[4] = {c[1], cjp, c[1], cjp};
+  const R wq[4] = {b1 * b2, b1 * del[1], del[0] * b2, del[0] * del[1]};
+  const PT* base = s.prim + (size_t)leaf * s.cells * kNPrim;
+#pragma unroll
+  for (int a = 0; a < kNPrim; a++) q[a] = R(0);
+#pragma unroll
+  for (int z = 0; z < 2; z++) {
+    const int ck = z ? ckp : c[2];
+    const R wz = z ? del[2] : b3;
+#pragma unroll
+    for (int n = 0; n < 4; n++) {
+      const PT* p = base + (size_t)(ci[n] + cj[n] * nx0 + ck * nx01) * kNPrim;
+      R v[kNPrim];
+#if defined(__CUDA_ARCH__)
+      if constexpr (sizeof(PT) == 4) {
+        const float4 lo4 = __ldg(reinterpret_cast<const float4*>(p));
+        const float4 hi4 = __ldg(reinterpret_cast<const float4*>(p) + 1);
+        v[0] = lo4.x; v[1] = lo4.y; v[2] = lo4.z; v[3] = lo4.w;
+        v[4] = hi4.x; v[5] = hi4.y; v[6] = hi4.z; v[7] = hi4.w;
+      } else {
+        const double2* p2 = reinterpret_cast<const double2*>(p);
+#pragma unroll
+        for (int h = 0; h < 4; h++) {
+          const double2 t = __ldg(p2 + h);
+          v[2 * h] = R(t.x);
+          v[2 * h + 1] = R(t.y);
+        }
+      }
+#else
+      for (int a = 0; a < kNPrim; a++) v[a] = R(p[a]);
+#endif
+      const R w = wq[n] * wz;
+#pragma unroll
+      for (int a = 0; a < kNPrim; a++) q[a] += v[a] * w;
+    }
+  }
+}
+
+// Fluid 4-velocity, magnetic 4-vector, |B| [G], n_e and Theta_e from the interpolated primitives; returns whether
+// the point emits (sampler.hpp:305-376).  g / u: metric at x.
+template <class R>
+PHX_HD bool derive_fluid(const PlasmaView<R>& pv, R gam, R r, const Cov<R>& g, const Contra<R>& u, const R q[kNPrim],
+                         Fluid<R>* fl) {
+  const R smalll = R(1e-6);
+  const R rho = q[kRho], uu = q[kUU];
+  fl->n_e = rho * pv.Ne + smalll;
+  const R shift1 = u.t1 / (-u.tt);
+  const R alpha = R(1) / sqrt_t(-u.tt);
+  const R gv1 = q[kU1], gv2 = q[kU2], gv3 = q[kU3];
+  const R gvv = g.x11 * gv1 * gv1 + R(2) * g.x13 * gv1 * gv3 + g.x22 * gv2 * gv2 + g.x33 * gv3 * gv3;
+  const R lfac = sqrt_t(gvv + R(1));
+  const R V1 = gv1 / lfac, V2 = gv2 / lfac, V3 = gv3 / lfac;
+  const R ut = lfac / alpha;
+  fl->U[0] = ut;
+  fl->U[1] = V1 * lfac - shift1 * ut;
+  fl->U[2] = V2 * lfac;
+  fl->U[3] = V3 * lfac;
+  const R Bp1 = q[kB1], Bp2 = q[kB2], Bp3 = q[kB3];
+  // B^t = lfac (gamma_ij Bp^i V^j) / alpha
+  const R BV = Bp1 * (g.x11 * V1 + g.x13 * V3) + Bp2 * (g.x22 * V2) + Bp3 * (g.x13 * V1 + g.x33 * V3);
+  fl->B[0] = lfac * BV / alpha;
+  fl->B[1] = (Bp1 + alpha * fl->B[0] * fl->U[1]) / lfac;
+  fl->B[2] = (Bp2 + alpha * fl->B[0] * fl->U[2]) / lfac;
+  fl->B[3] = (Bp3 + alpha * fl->B[0] * fl->U[3]) / lfac;
+  const R Bsq = fabs_t(dot(g, fl->B, fl->B)) + smalll;
+  fl->Bmag = sqrt_t(Bsq) * pv.Bu;
+  const R beta = uu * (gam - R(1)) / (R(0.5) * (Bsq + smalll));
+  const R bb = beta * pv.ibc;
+  const R b2 = bb * bb;
+  const R trat = pv.rhigh * b2 / (R(1) + b2) + pv.rlow / (R(1) + b2);
+  const R te_unit = R(1.0 / 3.0 * (cgs::m_proton / cgs::m_electron)) / (trat + R(1));
+  fl->theta_e = (uu / rho) * te_unit;
+  if ((Bsq / (rho + R(1e-20)) > pv.sigma_cut) || r > pv.rt_outer || fl->theta_e > pv.thetae_max ||
+      fl->theta_e < pv.thetae_min) {
+    fl->n_e = R(0);
+    return false;
+  }
+  return true;
+}
+
+}  // namespace phx

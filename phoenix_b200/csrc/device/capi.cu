@@ -1,0 +1,449 @@
+// The extern "C" boundary (include/phoenix_b200.h): snapshot residency, render launches, errors.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <cmath>
+#include <exception>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../../include/phoenix_b200.h"
+#include "../host/render_setup.hpp"
+#include "../host/snapshot.hpp"
+#include "march.cuh"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+struct CudaError : std::runtime_error {
+  explicit CudaError(const std::string& m) : std::runtime_error(m) {}
+};
+
+void ck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <class T>
+T* dev_upload(const T* host, size_t n, std::vector<void*>& owned) {
+  T* d = nullptr;
+  ck(cudaMalloc((void**)&d, std::max<size_t>(n, 1) * sizeof(T)), "cudaMalloc");
+  owned.push_back(d);
+  if (n) ck(cudaMemcpy(d, host, n * sizeof(T), cudaMemcpyHostToDevice), "cudaMemcpy H2D");
+  return d;
+}
+
+// Device workspace of the synchronous render entry (grown on demand, reused across calls).
+struct Workspace {
+  int32_t* jobs = nullptr;
+  size_t jobs_cap = 0;
+  PhxFreqOut* res = nullptr;
+  size_t res_cap = 0;
+  unsigned long long* counters = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  ~Workspace() {
+    cudaFree(jobs);
+    cudaFree(res);
+    cudaFree(counters);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+  }
+};
+
+}  // namespace
+
+struct PhxHostSnapshot {
+  phx::HostSnapshot h;
+  std::vector<const int32_t*> maps;
+};
+
+struct PhxSnapshot {
+  int device = 0;
+  int sms = 0;
+  char device_name[256] = {0};
+  int32_t nleafs = 0, nlevels = 0, cells = 0;
+  int32_t nx[3] = {0, 0, 0}, ng[3] = {0, 0, 0}, fd[3] = {0, 0, 0};
+  double a = 0, hslope = 0, gam = 0;
+  double x_lo[3] = {0, 0, 0}, x_hi[3] = {0, 0, 0};
+  float *lb_f = nullptr, *dxc_f = nullptr, *prim_f = nullptr;
+  double *lb_d = nullptr, *dxc_d = nullptr, *prim_d = nullptr;
+  int32_t* fmap = nullptr;
+  int64_t bytes = 0;
+  std::vector<void*> owned;
+  Workspace ws;
+  cudaStream_t stream = nullptr;
+  ~PhxSnapshot() {
+    if (stream) cudaStreamDestroy(stream);
+    for (void* p : owned) cudaFree(p);
+  }
+};
+
+namespace {
+
+template <class R, class PT>
+phx::SnapView<R, PT> snap_view(const PhxSnapshot* s, const R* lb, const R* dxc, const PT* prim) {
+  phx::SnapView<R, PT> v;
+  v.lb = lb;
+  v.dxc = dxc;
+  v.prim = prim;
+  v.fmap = s->fmap;
+  for (int d = 0; d < 3; d++) {
+    v.fd[d] = s->fd[d];
+    v.nx[d] = s->nx[d];
+    v.x_lo[1 + d] = R(s->x_lo[d]);
+    v.x_hi[1 + d] = R(s->x_hi[d]);
+    v.w0[d] = R((s->x_hi[d] - s->x_lo[d]) / s->ng[d]);
+  }
+  v.x_lo[0] = v.x_hi[0] = R(0);
+  v.nleafs = s->nleafs;
+  v.nlevels = s->nlevels;
+  v.cells = s->cells;
+  v.a = R(s->a);
+  v.hs = R(s->hslope);
+  v.gam = R(s->gam);
+  return v;
+}
+
+template <phx::Mode M, class PT>
+cudaError_t launch_mode(PhxSnapshot* s, const PhxRenderParams& p, const typename phx::Policy<M>::R* lb,
+                        const typename phx::Policy<M>::R* dxc, const PT* prim, const int32_t* d_jobs, int64_t njobs,
+                        PhxFreqOut* d_res, int32_t* d_pixstats, uint64_t* d_counters, cudaStream_t st,
+                        phx::LaunchShape* shape) {
+  using R = typename phx::Policy<M>::R;
+  phx::MarchArgs<R, PT> A;
+  A.snap = snap_view<R, PT>(s, lb, dxc, prim);
+  A.rc = phx::make_consts<R>(p, s->a, s->hslope);
+  A.jobs = d_jobs;
+  A.njobs = njobs;
+  A.out = reinterpret_cast<double*>(d_res);
+  A.pixstats = d_pixstats;
+  A.counters = reinterpret_cast<unsigned long long*>(d_counters);
+  A.period = p.period > 0 ? p.period : 1;
+  return phx::launch_march<M, PT>(A, s->sms, p.blocks_per_sm, st, shape);
+}
+
+cudaError_t dispatch(PhxSnapshot* s, const PhxRenderParams& p, const int32_t* d_jobs, int64_t njobs, PhxFreqOut* d_res,
+                     int32_t* d_pixstats, uint64_t* d_counters, cudaStream_t st, phx::LaunchShape* shape) {
+  switch (p.precision) {
+    case PHX_PREC_FP32:
+      return launch_mode<phx::Mode::kFP32, float>(s, p, s->lb_f, s->dxc_f, s->prim_f, d_jobs, njobs, d_res, d_pixstats,
+                                                  d_counters, st, shape);
+    case PHX_PREC_MIXED:
+      return launch_mode<phx::Mode::kMixed, float>(s, p, s->lb_f, s->dxc_f, s->prim_f, d_jobs, njobs, d_res,
+                                                   d_pixstats, d_counters, st, shape);
+    case PHX_PREC_FP64:
+      if (s->prim_d)
+        return launch_mode<phx::Mode::kFP64, double>(s, p, s->lb_d, s->dxc_d, s->prim_d, d_jobs, njobs, d_res,
+                                                     d_pixstats, d_counters, st, shape);
+      return launch_mode<phx::Mode::kFP64, float>(s, p, s->lb_d, s->dxc_d, s->prim_f, d_jobs, njobs, d_res,
+                                                  d_pixstats, d_counters, st, shape);
+  }
+  return cudaErrorInvalidValue;
+}
+
+void validate_desc(const PhxSnapshotDesc* d) {
+  auto bad = [](const std::string& m) { throw std::invalid_argument(m); };
+  if (!d) bad("null snapshot descriptor");
+  if (d->nleafs < 1) bad("nleafs must be >= 1");
+  if (d->nlevels < 1 || d->nlevels > PHX_MAX_LEVELS) bad("nlevels must be in 1..16");
+  for (int k = 0; k < 3; k++) {
+    if (d->nx[k] < 1 || d->ng[k] < 1) bad("nx and ng must be positive");
+    if (!(d->x_hi[k] > d->x_lo[k])) bad("empty domain");
+  }
+  if (!d->lb || !d->dxc || !d->prim_f32 || !d->level_map) bad("lb, dxc, prim_f32 and level_map are required");
+  if (!(std::fabs(d->a) < 1.0)) bad("spin must satisfy |a| < 1");
+  const size_t top = (size_t)1 << (d->nlevels - 1);
+  const size_t slots = d->ng[0] * top * d->ng[1] * top * d->ng[2] * top;
+  if (slots > ((size_t)1 << 31)) bad("finest-level leaf map too large (> 2^31 slots)");
+  for (int L = 0; L < d->nlevels; L++) {
+    if (!d->level_map[L]) bad("level_map[" + std::to_string(L) + "] is null");
+    const size_t n = ((size_t)d->ng[0] << L) * ((size_t)d->ng[1] << L) * ((size_t)d->ng[2] << L);
+    for (size_t t = 0; t < n; t++) {
+      const int32_t v = d->level_map[L][t];
+      if (v < -1 || v >= d->nleafs) bad("level_map holds a leaf id out of range");
+    }
+  }
+}
+
+PhxSnapshot* create_snapshot(const PhxSnapshotDesc* d, int32_t flags) {
+  validate_desc(d);
+  auto s = std::make_unique<PhxSnapshot>();
+  ck(cudaGetDevice(&s->device), "cudaGetDevice");
+  cudaDeviceProp prop;
+  ck(cudaGetDeviceProperties(&prop, s->device), "cudaGetDeviceProperties");
+  s->sms = prop.multiProcessorCount;
+  std::snprintf(s->device_name, sizeof s->device_name, "%s (sm_%d%d)", prop.name, prop.major, prop.minor);
+  s->nleafs = d->nleafs;
+  s->nlevels = d->nlevels;
+  s->cells = d->nx[0] * d->nx[1] * d->nx[2];
+  s->a = d->a;
+  s->hslope = d->hslope;
+  s->gam = d->gam;
+  for (int k = 0; k < 3; k++) {
+    s->nx[k] = d->nx[k];
+    s->ng[k] = d->ng[k];
+    s->fd[k] = d->ng[k] << (d->nlevels - 1);
+    s->x_lo[k] = d->x_lo[k];
+    s->x_hi[k] = d->x_hi[k];
+  }
+  const size_t n3 = 3 * (size_t)d->nleafs;
+  std::vector<float> lbf(n3), dxf(n3);
+  for (size_t t = 0; t < n3; t++) {
+    lbf[t] = (float)d->lb[t];
+    dxf[t] = (float)d->dxc[t];
+  }
+  std::vector<std::vector<int32_t>> maps(d->nlevels);
+  for (int L = 0; L < d->nlevels; L++) {
+    const size_t n = ((size_t)d->ng[0] << L) * ((size_t)d->ng[1] << L) * ((size_t)d->ng[2] << L);
+    maps[L].assign(d->level_map[L], d->level_map[L] + n);
+  }
+  const std::vector<int32_t> flat = phx::flatten_level_maps(maps, d->ng, d->nlevels);
+  const size_t nprim = (size_t)d->nleafs * s->cells * phx::kNPrim;
+  s->lb_f = dev_upload(lbf.data(), n3, s->owned);
+  s->dxc_f = dev_upload(dxf.data(), n3, s->owned);
+  s->lb_d = dev_upload(d->lb, n3, s->owned);
+  s->dxc_d = dev_upload(d->dxc, n3, s->owned);
+  s->prim_f = dev_upload(d->prim_f32, nprim, s->owned);
+  if ((flags & PHX_SNAP_F64_PRIMS) && d->prim_f64) s->prim_d = dev_upload(d->prim_f64, nprim, s->owned);
+  s->fmap = dev_upload(flat.data(), flat.size(), s->owned);
+  s->bytes = (int64_t)(n3 * (2 * sizeof(float) + 2 * sizeof(double)) + nprim * sizeof(float) +
+                       (s->prim_d ? nprim * sizeof(double) : 0) + flat.size() * sizeof(int32_t));
+  ck(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  return s.release();
+}
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    return f();
+  } catch (const CudaError& e) {
+    return fail(PHX_E_CUDA, e.what());
+  } catch (const std::invalid_argument& e) {
+    return fail(PHX_E_INVALID, e.what());
+  } catch (const std::bad_alloc&) {
+    return fail(PHX_E_INVALID, "host allocation failed");
+  } catch (const std::exception& e) {
+    return fail(PHX_E_IO, e.what());
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+void phx_default_params(PhxRenderParams* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof *p);
+  p->inclination = 50.0;
+  p->img_width = p->img_height = 200;
+  p->fov_x = p->fov_y = 40.0;
+  p->r_cam = 1e4;
+  p->t_init = 0.0;
+  p->nfreqs = 1;
+  p->frequencies[0] = 230e9;
+  p->mass = 4.14e6;
+  p->distance = 8.127;
+  p->stepsize = 0.01;
+  p->max_steps = 10000;
+  p->horizon_margin = 0.01;
+  p->max_order = 100;
+  p->m_unit = 1e18;
+  p->r_low = p->r_high = 1.0;
+  p->beta_c = 1.0;
+  p->sigma_cut = 1.0;
+  p->thetae_min = 1e-3;
+  p->thetae_max = 100.0;
+  p->rt_outer = 50.0;
+  p->precision = PHX_PREC_FP32;
+}
+
+int phx_snapshot_create(const PhxSnapshotDesc* desc, int32_t flags, PhxSnapshot** out) {
+  return guarded([&]() -> int {
+    if (!out) throw std::invalid_argument("null output handle");
+    *out = create_snapshot(desc, flags);
+    return PHX_OK;
+  });
+}
+
+int phx_bhac_read(const char* dump_file, const char* grid_file, const PhxReadOptions* opt, int32_t flags,
+                  PhxHostSnapshot** out) {
+  return guarded([&]() -> int {
+    if (!out || !dump_file || !grid_file) throw std::invalid_argument("null argument");
+    phx::SnapshotOptions o;
+    if (opt) {
+      o.nspin = opt->nspin;
+      o.bpol = opt->bpol;
+      o.sfc = opt->sfc != 0;
+      o.nlevels = opt->nlevels;
+    }
+    o.keep_f64 = (flags & PHX_SNAP_F64_PRIMS) != 0;
+    auto hs = std::make_unique<PhxHostSnapshot>();
+    hs->h = phx::load_bhac(dump_file, grid_file, o);
+    for (int L = 0; L < hs->h.nlevels; L++) hs->maps.push_back(hs->h.level_map[L].data());
+    *out = hs.release();
+    return PHX_OK;
+  });
+}
+
+int phx_bhac_describe(const PhxHostSnapshot* hs, PhxSnapshotDesc* d) {
+  return guarded([&]() -> int {
+    if (!hs || !d) throw std::invalid_argument("null argument");
+    const phx::HostSnapshot& h = hs->h;
+    std::memset(d, 0, sizeof *d);
+    d->nleafs = h.nleafs;
+    d->nlevels = h.nlevels;
+    for (int k = 0; k < 3; k++) {
+      d->nx[k] = h.nx[k];
+      d->ng[k] = h.ng[k];
+      d->x_lo[k] = h.x_lo[k];
+      d->x_hi[k] = h.x_hi[k];
+    }
+    d->a = h.a;
+    d->hslope = h.hslope;
+    d->gam = h.gam;
+    d->lb = h.lb.data();
+    d->dxc = h.dxc.data();
+    d->prim_f32 = h.prim_f32.data();
+    d->prim_f64 = h.prim_f64.empty() ? nullptr : h.prim_f64.data();
+    d->level_map = hs->maps.data();
+    return PHX_OK;
+  });
+}
+
+void phx_bhac_free(PhxHostSnapshot* h) { delete h; }
+
+int phx_snapshot_load(const char* dump_file, const char* grid_file, const PhxReadOptions* opt, int32_t flags,
+                      PhxSnapshot** out) {
+  return guarded([&]() -> int {
+    if (!out) throw std::invalid_argument("null output handle");
+    PhxHostSnapshot* hs = nullptr;
+    const int rc = phx_bhac_read(dump_file, grid_file, opt, flags, &hs);
+    if (rc != PHX_OK) return rc;
+    std::unique_ptr<PhxHostSnapshot> guard(hs);
+    PhxSnapshotDesc d;
+    phx_bhac_describe(hs, &d);
+    *out = create_snapshot(&d, flags);
+    return PHX_OK;
+  });
+}
+
+void phx_snapshot_destroy(PhxSnapshot* s) { delete s; }
+
+int64_t phx_snapshot_bytes(const PhxSnapshot* s) { return s ? s->bytes : 0; }
+
+int phx_schedule_morton(int32_t W, int32_t H, int32_t* jobs) {
+  return guarded([&]() -> int {
+    if (!jobs || W < 1 || H < 1 || (long long)W * H > (1LL << 31) - 1) throw std::invalid_argument("bad job list");
+    std::vector<std::pair<unsigned long long, int32_t>> keyed((size_t)W * H);
+    for (int i = 0; i < W; i++)
+      for (int j = 0; j < H; j++) {
+        unsigned long long z = 0;
+        for (int b = 0; b < 16; b++)
+          z |= ((unsigned long long)((i >> b) & 1) << (2 * b)) | ((unsigned long long)((j >> b) & 1) << (2 * b + 1));
+        keyed[(size_t)i * H + j] = {z, i * H + j};
+      }
+    std::sort(keyed.begin(), keyed.end());
+    for (size_t n = 0; n < keyed.size(); n++) jobs[n] = keyed[n].second;
+    return PHX_OK;
+  });
+}
+
+int phx_render_async(PhxSnapshot* s, const PhxRenderParams* p, const int32_t* d_jobs, int64_t njobs,
+                     PhxFreqOut* d_res, int32_t* d_pixstats, uint64_t* d_counters, void* stream) {
+  return guarded([&]() -> int {
+    if (!s || !p || !d_res || !d_counters || (njobs > 0 && !d_jobs)) throw std::invalid_argument("null argument");
+    phx::check_params(*p);
+    if (njobs < 0 || njobs > (int64_t)p->img_width * p->img_height) throw std::invalid_argument("njobs out of range");
+    phx::LaunchShape shape;
+    ck(dispatch(s, *p, d_jobs, njobs, d_res, d_pixstats, d_counters, (cudaStream_t)stream, &shape), "render launch");
+    return PHX_OK;
+  });
+}
+
+int phx_render(PhxSnapshot* s, const PhxRenderParams* p, const int32_t* jobs, int64_t njobs, PhxFreqOut* res,
+               PhxRenderInfo* info) {
+  return guarded([&]() -> int {
+    if (!s || !p || !res) throw std::invalid_argument("null argument");
+    phx::check_params(*p);
+    const auto t0 = std::chrono::steady_clock::now();
+    const int64_t npix = (int64_t)p->img_width * p->img_height;
+    std::vector<int32_t> all;
+    if (!jobs) {
+      all.resize(npix);
+      if (phx_schedule_morton(p->img_width, p->img_height, all.data()) != PHX_OK) throw std::runtime_error(g_err);
+      jobs = all.data();
+      njobs = npix;
+    }
+    if (njobs < 0 || njobs > npix) throw std::invalid_argument("njobs out of range");
+    for (int64_t n = 0; n < njobs; n++)
+      if (jobs[n] < 0 || jobs[n] >= npix) throw std::invalid_argument("job index out of range");
+    Workspace& w = s->ws;
+    const size_t nres = (size_t)npix * p->nfreqs;
+    if (w.jobs_cap < (size_t)njobs) {
+      cudaFree(w.jobs);
+      w.jobs = nullptr;
+      ck(cudaMalloc((void**)&w.jobs, std::max<size_t>(njobs, 1) * sizeof(int32_t)), "cudaMalloc jobs");
+      w.jobs_cap = std::max<size_t>(njobs, 1);
+    }
+    if (w.res_cap < nres) {
+      cudaFree(w.res);
+      w.res = nullptr;
+      ck(cudaMalloc((void**)&w.res, nres * sizeof(PhxFreqOut)), "cudaMalloc res");
+      w.res_cap = nres;
+    }
+    if (!w.counters) ck(cudaMalloc((void**)&w.counters, phx::kNumCounters * sizeof(unsigned long long)), "cudaMalloc");
+    if (!w.e0) ck(cudaEventCreate(&w.e0), "cudaEventCreate");
+    if (!w.e1) ck(cudaEventCreate(&w.e1), "cudaEventCreate");
+    cudaStream_t st = s->stream;
+    ck(cudaMemcpyAsync(w.jobs, jobs, njobs * sizeof(int32_t), cudaMemcpyHostToDevice, st), "H2D jobs");
+    // pixels outside the job list keep the caller's values, as in the reference (res is uploaded and read back)
+    if (njobs < npix) ck(cudaMemcpyAsync(w.res, res, nres * sizeof(PhxFreqOut), cudaMemcpyHostToDevice, st), "H2D res");
+    ck(cudaMemsetAsync(w.counters, 0, phx::kNumCounters * sizeof(unsigned long long), st), "memset");
+    const double upload_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    phx::LaunchShape shape;
+    ck(cudaEventRecord(w.e0, st), "event");
+    ck(dispatch(s, *p, w.jobs, njobs, w.res, nullptr, reinterpret_cast<uint64_t*>(w.counters), st, &shape),
+       "render launch");
+    ck(cudaEventRecord(w.e1, st), "event");
+    unsigned long long ctr[phx::kNumCounters];
+    ck(cudaMemcpyAsync(res, w.res, nres * sizeof(PhxFreqOut), cudaMemcpyDeviceToHost, st), "D2H res");
+    ck(cudaMemcpyAsync(ctr, w.counters, sizeof ctr, cudaMemcpyDeviceToHost, st), "D2H counters");
+    ck(cudaStreamSynchronize(st), "render");
+    if (info) {
+      std::memset(info, 0, sizeof *info);
+      std::snprintf(info->device, sizeof info->device, "%s", s->device_name);
+      info->sms = s->sms;
+      info->blocks = shape.grid;
+      info->block = shape.block;
+      info->regs = shape.regs;
+      info->local_bytes = shape.local_bytes;
+      float ms = 0.f;
+      ck(cudaEventElapsedTime(&ms, w.e0, w.e1), "event time");
+      info->kernel_s = ms * 1e-3;
+      info->upload_s = upload_s;
+      info->steps = (int64_t)ctr[phx::kCtrSteps];
+      info->nplasma = (int64_t)ctr[phx::kCtrPlasma];
+      info->bad = (int64_t)ctr[phx::kCtrBad];
+      info->scans = (int64_t)ctr[phx::kCtrScans];
+      info->fp64_steps = (int64_t)ctr[phx::kCtrFp64Steps];
+      info->fp64_ops = (int64_t)ctr[phx::kCtrFp64Ops];
+    }
+    return PHX_OK;
+  });
+}
+
+const char* phx_last_error(void) { return g_err.c_str(); }
+
+const char* phx_version(void) { return "phoenix-b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

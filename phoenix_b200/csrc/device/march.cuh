@@ -1,0 +1,127 @@
+// The fused raymarch kernel: a persistent grid of warps, one ray per lane, with warp-level lane refill.
+//
+// Every pass of the march loop is one Ray::advance() per live lane (geodesic step + leaf lookups + the plasma
+// stage of the previous sample + its transfer operator for every frequency).  Every `period` passes each warp
+// collects its finished lanes with a ballot, takes that many pixel jobs from the device queue with one atomic,
+// and starts the new rays in those lanes (prefix-popcount ranks), so a warp never waits for its longest ray:
+// the reference kernel (src/device/kernel.cu:70-100) runs each pixel's whole inner loop per lane, and a lane that
+// finished early idles until its warp's longest ray ends.
+//
+// Device buffers a launch touches: the snapshot pool and job list (read), the FreqOut image (written once per
+// pixel), optional per-pixel statistics, and a 16-word counter block (queue head + diagnostic sums).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "../core/ray.cuh"
+
+namespace phx {
+
+enum CounterSlot {
+  kCtrQueue = 0,
+  kCtrSteps = 1,
+  kCtrPlasma = 2,
+  kCtrBad = 3,
+  kCtrScans = 4,
+  kCtrFp64Steps = 5,
+  kCtrFp64Ops = 6,
+  kCtrRays = 7,
+  kNumCounters = 16
+};
+
+template <class R, class PT>
+struct MarchArgs {
+  SnapView<R, PT> snap;
+  RenderConsts<R> rc;
+  const int32_t* jobs;
+  int64_t njobs;
+  double* out;
+  int32_t* pixstats;
+  unsigned long long* counters;
+  int32_t period;
+};
+
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <Mode M, class PT, int NF, int kBlock, int kMinBlocks>
+__global__ void __launch_bounds__(kBlock, kMinBlocks)
+    k_march(const __grid_constant__ MarchArgs<typename Policy<M>::R, PT> A) {
+  using RayT = Ray<M, PT, NF>;
+  const unsigned lane = threadIdx.x & 31u;
+  RayT ray;
+  RayCounters ctr{};
+  unsigned long long steps = 0, nplasma = 0, bad = 0, rays = 0;
+  bool live = false, drained = false;
+  for (;;) {
+    if (!drained) {
+      const unsigned idle = __ballot_sync(0xffffffffu, !live);
+      if (idle) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(&A.counters[kCtrQueue], (unsigned long long)__popc(idle));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= (unsigned long long)A.njobs) drained = true;
+        if (!live) {
+          const unsigned long long job = base + __popc(idle & ((1u << lane) - 1u));
+          if (job < (unsigned long long)A.njobs) {
+            const int32_t pix = A.jobs[job];
+            // a job outside the image is skipped, never written (the host checks job lists it uploads itself)
+            if (pix >= 0 && pix < A.rc.W * A.rc.H) {
+              ray.init(A.snap, A.rc, pix);
+              live = true;
+            }
+          }
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, live)) break;
+    for (int it = 0; it < A.period; it++) {
+      if (live) {
+        live = ray.advance(A.snap, A.rc, ctr);
+        if (!live) {
+          ray.write(A.out, A.rc.nfreqs);
+          if (A.pixstats) {
+            int32_t* ps = A.pixstats + 3 * (size_t)ray.pix;
+            ps[0] = ray.steps;
+            ps[1] = ray.nplasma;
+            ps[2] = ray.bad;
+          }
+          steps += (unsigned)ray.steps;
+          nplasma += (unsigned)ray.nplasma;
+          bad += (unsigned)ray.bad;
+          rays++;
+        }
+      }
+    }
+  }
+  steps = warp_sum_u64(steps);
+  nplasma = warp_sum_u64(nplasma);
+  bad = warp_sum_u64(bad);
+  rays = warp_sum_u64(rays);
+  const unsigned long long scans = warp_sum_u64(ctr.scans);
+  const unsigned long long f64s = warp_sum_u64(ctr.fp64_steps);
+  const unsigned long long f64o = warp_sum_u64(ctr.fp64_ops);
+  if (lane == 0) {
+    atomicAdd(&A.counters[kCtrSteps], steps);
+    atomicAdd(&A.counters[kCtrPlasma], nplasma);
+    atomicAdd(&A.counters[kCtrBad], bad);
+    atomicAdd(&A.counters[kCtrRays], rays);
+    if (scans) atomicAdd(&A.counters[kCtrScans], scans);
+    if (f64s) atomicAdd(&A.counters[kCtrFp64Steps], f64s);
+    if (f64o) atomicAdd(&A.counters[kCtrFp64Ops], f64o);
+  }
+}
+
+// Launch entry per (mode, prim type): picks the frequency-slot instantiation and the launch shape.
+struct LaunchShape {
+  int block, grid, regs, local_bytes, blocks_per_sm;
+};
+
+template <Mode M, class PT>
+cudaError_t launch_march(const MarchArgs<typename Policy<M>::R, PT>& args, int sms, int blocks_per_sm,
+                         cudaStream_t stream, LaunchShape* shape);
+
+}  // namespace phx

@@ -1,0 +1,153 @@
+"""ctypes binding of the C ABI in include/phoenix_b200.h (libphoenix_b200.so, built in-tree by phoenix_b200.build).
+
+There is no fallback: if the library is missing or cannot be loaded, importing the render entry points raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "_build", "libphoenix_b200.so")
+
+MAX_FREQS = 32
+MAX_LEVELS = 16
+
+PHX_OK, PHX_E_INVALID, PHX_E_IO, PHX_E_CUDA, PHX_E_TIMEOUT, PHX_E_UNSUPPORTED = 0, -1, -2, -3, -4, -5
+PREC_FP32, PREC_FP64, PREC_MIXED = 0, 1, 2
+PRECISIONS = {"fp32": PREC_FP32, "fp64": PREC_FP64, "mixed": PREC_MIXED}
+SNAP_F64_PRIMS = 1
+NUM_COUNTERS = 16
+CTR = dict(queue=0, steps=1, nplasma=2, bad=3, scans=4, fp64_steps=5, fp64_ops=6, rays=7)
+
+# Every symbol include/phoenix_b200.h declares.
+EXPORTS = ["phx_default_params", "phx_snapshot_create", "phx_snapshot_load", "phx_snapshot_destroy",
+           "phx_bhac_read", "phx_bhac_describe", "phx_bhac_free", "phx_snapshot_bytes", "phx_schedule_morton", "phx_render", "phx_render_async", "phx_last_error",
+           "phx_version"]
+
+
+class PhxFreqOut(C.Structure):
+    _fields_ = [("IQUV", C.c_double * 4), ("tau", C.c_double), ("tauF", C.c_double)]
+
+
+class PhxSnapshotDesc(C.Structure):
+    _fields_ = [
+        ("nleafs", C.c_int32), ("nx", C.c_int32 * 3), ("ng", C.c_int32 * 3), ("nlevels", C.c_int32),
+        ("a", C.c_double), ("hslope", C.c_double), ("gam", C.c_double),
+        ("x_lo", C.c_double * 3), ("x_hi", C.c_double * 3),
+        ("lb", C.c_void_p), ("dxc", C.c_void_p), ("prim_f32", C.c_void_p), ("prim_f64", C.c_void_p),
+        ("level_map", C.c_void_p),
+    ]
+
+
+class PhxReadOptions(C.Structure):
+    _fields_ = [("nspin", C.c_int32), ("bpol", C.c_int32), ("sfc", C.c_int32), ("nlevels", C.c_int32)]
+
+
+class PhxRenderParams(C.Structure):
+    _fields_ = [
+        ("inclination", C.c_double), ("fov_x", C.c_double), ("fov_y", C.c_double), ("r_cam", C.c_double),
+        ("t_init", C.c_double), ("pa", C.c_double), ("phi", C.c_double),
+        ("img_width", C.c_int32), ("img_height", C.c_int32), ("nfreqs", C.c_int32),
+        ("frequencies", C.c_double * MAX_FREQS),
+        ("mass", C.c_double), ("distance", C.c_double),
+        ("stepsize", C.c_double), ("max_steps", C.c_int32), ("horizon_margin", C.c_double), ("max_order", C.c_int32),
+        ("m_unit", C.c_double), ("r_low", C.c_double), ("r_high", C.c_double), ("beta_c", C.c_double),
+        ("sigma_cut", C.c_double), ("thetae_min", C.c_double), ("thetae_max", C.c_double), ("rt_outer", C.c_double),
+        ("precision", C.c_int32), ("r_fp64", C.c_double), ("tau_fp64", C.c_double),
+        ("block", C.c_int32), ("period", C.c_int32), ("blocks_per_sm", C.c_int32),
+    ]
+
+
+class PhxRenderInfo(C.Structure):
+    _fields_ = [
+        ("device", C.c_char * 256), ("sms", C.c_int32), ("blocks", C.c_int32), ("block", C.c_int32),
+        ("regs", C.c_int32), ("local_bytes", C.c_int32), ("upload_s", C.c_double), ("kernel_s", C.c_double),
+        ("steps", C.c_int64), ("nplasma", C.c_int64), ("bad", C.c_int64), ("scans", C.c_int64),
+        ("fp64_steps", C.c_int64), ("fp64_ops", C.c_int64),
+    ]
+
+    def as_dict(self):
+        d = {name: getattr(self, name) for name, _ in self._fields_}
+        d["device"] = self.device.decode()
+        return d
+
+
+class PhxError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"phoenix_b200 error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """The loaded native library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} not found: build it with `python -m phoenix_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    P = C.POINTER
+    L.phx_default_params.argtypes = [P(PhxRenderParams)]
+    L.phx_default_params.restype = None
+    L.phx_snapshot_create.argtypes = [P(PhxSnapshotDesc), C.c_int32, P(C.c_void_p)]
+    L.phx_snapshot_load.argtypes = [C.c_char_p, C.c_char_p, P(PhxReadOptions), C.c_int32, P(C.c_void_p)]
+    L.phx_snapshot_destroy.argtypes = [C.c_void_p]
+    L.phx_snapshot_destroy.restype = None
+    L.phx_bhac_read.argtypes = [C.c_char_p, C.c_char_p, P(PhxReadOptions), C.c_int32, P(C.c_void_p)]
+    L.phx_bhac_describe.argtypes = [C.c_void_p, P(PhxSnapshotDesc)]
+    L.phx_bhac_free.argtypes = [C.c_void_p]
+    L.phx_bhac_free.restype = None
+    L.phx_snapshot_bytes.argtypes = [C.c_void_p]
+    L.phx_snapshot_bytes.restype = C.c_int64
+    L.phx_schedule_morton.argtypes = [C.c_int32, C.c_int32, C.c_void_p]
+    L.phx_render.argtypes = [C.c_void_p, P(PhxRenderParams), C.c_void_p, C.c_int64, C.c_void_p, P(PhxRenderInfo)]
+    L.phx_render_async.argtypes = [C.c_void_p, P(PhxRenderParams), C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_void_p]
+    L.phx_last_error.restype = C.c_char_p
+    L.phx_version.restype = C.c_char_p
+    for name in ("phx_snapshot_create", "phx_snapshot_load", "phx_bhac_read", "phx_bhac_describe", "phx_schedule_morton",
+                 "phx_render", "phx_render_async"):
+        getattr(L, name).restype = C.c_int
+    _lib = L
+    return L
+
+
+def check(code: int):
+    if code != PHX_OK:
+        raise PhxError(code, lib().phx_last_error().decode())
+
+
+def make_params(**kw) -> PhxRenderParams:
+    """Render parameters: the reference's config.toml defaults overridden by keyword (config key names;
+    `frequencies` is a sequence, `precision` one of fp32 / fp64 / mixed or a PREC_* code)."""
+    p = PhxRenderParams()
+    lib().phx_default_params(C.byref(p))
+    for k, v in kw.items():
+        if k == "frequencies" or k == "frequency":
+            fr = [float(v)] if np.isscalar(v) else [float(x) for x in v]
+            if not 1 <= len(fr) <= MAX_FREQS:
+                raise ValueError("1..32 frequencies")
+            p.nfreqs = len(fr)
+            for i, f in enumerate(fr):
+                p.frequencies[i] = f
+        elif k == "precision":
+            p.precision = PRECISIONS[v] if isinstance(v, str) else int(v)
+        elif k in ("img", "resolution"):
+            p.img_width = p.img_height = int(v)
+        else:
+            if not hasattr(p, k):
+                raise KeyError(f"unknown render parameter {k}")
+            setattr(p, k, v)
+    return p
+
+
+def schedule_morton(width: int, height: int) -> np.ndarray:
+    jobs = np.empty(width * height, dtype=np.int32)
+    check(lib().phx_schedule_morton(width, height, jobs.ctypes.data))
+    return jobs

@@ -1,0 +1,148 @@
+"""Parity of the sm_100a raymarch kernels with the FP64 oracle and the reference's golden outputs (needs a GPU).
+
+Tolerances (total flux relative to Stokes I of the same frequency; L1 relative over the image):
+  FP64   flux 1e-9, per-pixel L1 1e-8, step counts identical on >= 99.5% of the pixels
+  FP32   flux I <= 1e-4 and Q/U/V <= 1e-3 of I (the path's stated bar), L1 <= 1e-3
+  mixed  same bar as FP32
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import phoenix_b200 as P
+from tests.conftest import golden_arrays
+from tests.golden.cases import CASES, case_params
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": dict(flux=1e-9, l1=1e-8), "fp32": dict(flux=1e-4, pol=1e-3, l1=1e-3),
+       "mixed": dict(flux=1e-4, pol=1e-3, l1=1e-3)}
+
+
+@pytest.fixture(scope="module")
+def gpu_snapshots(snapshots):
+    out = {}
+    for name, (dump, grid, spec) in snapshots.items():
+        out[name] = P.Snapshot.load(dump, grid, nlevels=spec["nlevels"], sfc=spec["sfc"], f64_prims=True)
+    yield out
+    for s in out.values():
+        s.close()
+
+
+def render_case(snaps, name, precision, **over):
+    kw = case_params(name)
+    kw.update(over)
+    p = P.make_params(precision=precision, **kw)
+    res, info = snaps[CASES[name]["snapshot"]].render(p)
+    return res, info, p
+
+
+def flux_errors(res, ref, p):
+    f = P.flux(res, p)
+    g = P.flux(ref, p)
+    err = np.abs(f - g) / np.abs(g[:, :1])
+    return err  # [nfreqs, 4] relative to I
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "mixed"])
+def test_matches_oracle(gpu_snapshots, oracle_results, name, precision):
+    ref, st_ref, _ = oracle_results(name)
+    res, info, p = render_case(gpu_snapshots, name, precision)
+    assert info["bad"] == 0 or precision != "fp64"
+    err = flux_errors(res, ref, p)
+    l1 = np.abs(res[..., :4] - ref[..., :4]).sum() / np.abs(ref[..., :4]).sum()
+    t = TOL[precision]
+    if precision == "fp64":
+        assert err.max() <= t["flux"], err
+    else:
+        assert err[:, 0].max() <= t["flux"], err
+        assert err[:, 1:].max() <= t["pol"], err
+    assert l1 <= t["l1"], l1
+    assert np.isfinite(res).all()
+    # the march visits the same samples: total steps agree closely, and exactly per pixel at FP64
+    assert abs(info["steps"] - int(st_ref[..., 0].sum())) <= 0.002 * st_ref[..., 0].sum()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_fp64_steps_per_pixel(gpu_snapshots, oracle_results, snapshots, name):
+    """FP64 marches take the reference's steps and plasma segments pixel by pixel (pixel statistics via the async
+    entry point)."""
+    import torch
+    ref, st_ref, _ = oracle_results(name)
+    kw = case_params(name)
+    p = P.make_params(precision="fp64", **kw)
+    W, H, F = p.img_width, p.img_height, p.nfreqs
+    dev = torch.device("cuda")
+    jobs = torch.from_numpy(P.schedule_morton(W, H)).to(dev)
+    res = torch.zeros((W, H, F, 6), dtype=torch.float64, device=dev)
+    ps = torch.zeros((W, H, 3), dtype=torch.int32, device=dev)
+    ctr = torch.zeros(P.NUM_COUNTERS, dtype=torch.int64, device=dev)
+    snap = gpu_snapshots[CASES[name]["snapshot"]]
+    stream = torch.cuda.current_stream()
+    snap.render_async(p, jobs.data_ptr(), jobs.numel(), res.data_ptr(), ctr.data_ptr(), ps.data_ptr(),
+                      stream.cuda_stream)
+    torch.cuda.synchronize()
+    st = ps.cpu().numpy()
+    same = (st[..., 0] == st_ref[..., 0]) & (st[..., 1] == st_ref[..., 1])
+    assert same.mean() >= 0.995, same.mean()
+    assert int(ctr[P.CTR["rays"]]) == W * H
+    assert int(ctr[P.CTR["steps"]]) == int(st[..., 0].sum())
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_fp64_matches_reference_golden(gpu_snapshots, golden_meta, name):
+    """Against the reference's own FP64 output (committed fixture)."""
+    g = golden_arrays(name)["res_fp64"]
+    res, info, p = render_case(gpu_snapshots, name, "fp64")
+    assert flux_errors(res, g, p).max() <= 1e-9
+    assert info["steps"] == golden_meta["cases"][name]["reference"]["fp64"]["steps"] or \
+        abs(info["steps"] - golden_meta["cases"][name]["reference"]["fp64"]["steps"]) <= 0.002 * info["steps"]
+
+
+def test_job_subset_leaves_other_pixels(gpu_snapshots):
+    p = P.make_params(precision="fp32", **case_params("edge"))
+    W, H, F = p.img_width, p.img_height, p.nfreqs
+    full, _ = gpu_snapshots["small"].render(p)
+    sentinel = np.full((W, H, F, 6), -7.0)
+    jobs = np.array([0, 5, W * H - 1, 17], dtype=np.int32)
+    part, info = gpu_snapshots["small"].render(p, jobs=jobs, out=sentinel.copy())
+    flat_full, flat_part = full.reshape(W * H, F, 6), part.reshape(W * H, F, 6)
+    mask = np.zeros(W * H, bool)
+    mask[jobs] = True
+    assert np.array_equal(flat_part[mask], flat_full[mask])
+    assert np.all(flat_part[~mask] == -7.0)
+    empty, info0 = gpu_snapshots["small"].render(p, jobs=np.zeros(0, np.int32), out=sentinel.copy())
+    assert np.all(empty == -7.0) and info0["steps"] == 0
+
+
+def test_frequencies_are_independent(gpu_snapshots):
+    """A three-frequency render equals three single-frequency renders (per-frequency state only)."""
+    kw = case_params("thick")
+    multi, _ = gpu_snapshots["cfg1"].render(P.make_params(precision="fp64", **kw))
+    for f, nu in enumerate(kw["frequencies"]):
+        one = dict(kw)
+        one["frequencies"] = [nu]
+        single, _ = gpu_snapshots["cfg1"].render(P.make_params(precision="fp64", **one))
+        scale = np.abs(single).max()
+        assert np.abs(multi[:, :, f] - single[:, :, 0]).max() <= 1e-12 * scale
+
+
+@pytest.mark.parametrize("period,bps", [(1, 0), (4, 1), (16, 0)])
+def test_results_independent_of_launch_shape(gpu_snapshots, period, bps):
+    """Each ray's arithmetic does not depend on which lane or warp runs it: bit-identical images."""
+    kw = case_params("cfg1")
+    base, _ = gpu_snapshots["cfg1"].render(P.make_params(precision="fp32", **kw))
+    other, _ = gpu_snapshots["cfg1"].render(P.make_params(precision="fp32", period=period, blocks_per_sm=bps, **kw))
+    assert np.array_equal(base, other)
+
+
+def test_invalid_arguments_are_reported(gpu_snapshots):
+    p = P.make_params(img=0)
+    with pytest.raises(P.PhxError) as e:
+        gpu_snapshots["small"].render(p, out=np.zeros((0, 0, 1, 6)))
+    assert e.value.code == -1
+    p = P.make_params(img=8)
+    with pytest.raises(P.PhxError):
+        gpu_snapshots["small"].render(p, jobs=np.array([64], np.int32))
