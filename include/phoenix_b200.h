@@ -154,6 +154,21 @@ int phx_render(PhxSnapshot* s, const PhxRenderParams* p, const int32_t* jobs, in
 int phx_render_async(PhxSnapshot* s, const PhxRenderParams* p, const int32_t* d_jobs, int64_t njobs,
                      PhxFreqOut* d_res, int32_t* d_pixstats, uint64_t* d_counters, void* stream);
 
+/* No counterpart in the reference, whose device::render allocates on every call.  For callers that cannot call
+ * cudaMalloc -- a host application that owns all device memory through its own pool or arena, or a serving loop in
+ * which an allocation would synchronize the device and stall other streams -- this entry point allocates nothing:
+ * it stages `jobs` (host memory; pinned memory must stay valid until the stream has passed this call) and the
+ * kernel's scratch (work-queue head, counters) in a fixed library-owned device array of 256 bytes plus
+ * PHX_NOALLOC_MAX_JOBS job slots (4 MiB), which every GPU that loads the library holds until the process exits.
+ * d_res: device buffer of img_width * img_height * nfreqs records.  Asynchronous on `stream` (NULL = default).
+ * Rejects njobs > PHX_NOALLOC_MAX_JOBS with PHX_E_INVALID.  The first call on a device resolves the array's
+ * device address with that device current; make that first call before any stream capture.  All calls share the
+ * array (it keeps the last call's contents; the counter block is cleared before each launch), so calls that overlap
+ * on the GPU race. */
+#define PHX_NOALLOC_MAX_JOBS (1 << 20)
+int phx_render_noalloc(PhxSnapshot* s, const PhxRenderParams* p, const int32_t* jobs, int64_t njobs,
+                       PhxFreqOut* d_res, void* stream);
+
 /* Description of the last error on this host thread. */
 const char* phx_last_error(void);
 

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <exception>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -447,3 +448,71 @@ const char* phx_last_error(void) { return g_err.c_str(); }
 const char* phx_version(void) { return "phoenix-b200 0.1 (sm_100a)"; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------------------------
+// Rendering without any device allocation.
+//
+// Some callers cannot call cudaMalloc: a host application that owns all device memory through its own pool or arena
+// (so a library allocation would fragment it or fail its accounting), or a serving loop that must not let an
+// allocation synchronize the device and stall the other streams in flight.  phx_render_noalloc serves them: the
+// job list and the kernel's scratch (work-queue head and counter block) live in the fixed array below, which the
+// library's module holds on every GPU that loads it, until the process exits.  The caller passes the snapshot,
+// the parameters, the job list in host memory and the device result buffer; nothing else is allocated.
+//
+// Layout of the array: [0, 256) the 16-word counter block (word 0 = queue head), [256, 256 + 4 * kNoAllocMaxJobs)
+// the job list.  Every call shares it and it keeps the last call's contents: the counter block is cleared on the
+// stream before each launch, and calls that overlap on the GPU race on it.
+namespace {
+
+constexpr size_t kNoAllocHeader = 256;
+constexpr int64_t kNoAllocMaxJobs = PHX_NOALLOC_MAX_JOBS;
+constexpr size_t kNoAllocBytes = kNoAllocHeader + sizeof(int32_t) * (size_t)kNoAllocMaxJobs;
+static_assert(phx::kNumCounters * sizeof(unsigned long long) <= kNoAllocHeader, "counter block must fit the header");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device, resolved once per device (the symbol's host-side name
+// is only a stand-in and must never be passed to a kernel).
+void* noalloc_scratch(int device) {
+  if (device < 0 || device >= kNoAllocMaxDevices) throw std::invalid_argument("device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[device]) {
+    void* ptr = nullptr;
+    ck(cudaGetSymbolAddress(&ptr, g_noalloc_scratch), "cudaGetSymbolAddress");
+    g_noalloc_ptr[device] = ptr;
+  }
+  return g_noalloc_ptr[device];
+}
+
+}  // namespace
+
+extern "C" int phx_render_noalloc(PhxSnapshot* s, const PhxRenderParams* p, const int32_t* jobs, int64_t njobs,
+                                  PhxFreqOut* d_res, void* stream) {
+  return guarded([&]() -> int {
+    if (!s || !p || !d_res || (njobs > 0 && !jobs)) throw std::invalid_argument("null argument");
+    phx::check_params(*p);
+    if (njobs < 0) throw std::invalid_argument("njobs must be >= 0");
+    if (njobs > kNoAllocMaxJobs)
+      throw std::invalid_argument("njobs = " + std::to_string(njobs) + " exceeds the no-allocation limit of " +
+                                  std::to_string(kNoAllocMaxJobs) + " jobs (PHX_NOALLOC_MAX_JOBS)");
+    const int64_t npix = (int64_t)p->img_width * p->img_height;
+    for (int64_t n = 0; n < njobs; n++)
+      if (jobs[n] < 0 || jobs[n] >= npix) throw std::invalid_argument("job index out of range");
+    int device = 0;
+    ck(cudaGetDevice(&device), "cudaGetDevice");
+    if (device != s->device) throw std::invalid_argument("the snapshot lives on another device");
+    unsigned char* base = static_cast<unsigned char*>(noalloc_scratch(device));
+    uint64_t* counters = reinterpret_cast<uint64_t*>(base);
+    int32_t* d_jobs = reinterpret_cast<int32_t*>(base + kNoAllocHeader);
+    cudaStream_t st = (cudaStream_t)stream;
+    ck(cudaMemsetAsync(counters, 0, phx::kNumCounters * sizeof(unsigned long long), st), "memset scratch");
+    if (njobs > 0) ck(cudaMemcpyAsync(d_jobs, jobs, njobs * sizeof(int32_t), cudaMemcpyHostToDevice, st), "H2D jobs");
+    phx::LaunchShape shape;
+    ck(dispatch(s, *p, d_jobs, njobs, d_res, nullptr, counters, st, &shape), "render launch");
+    return PHX_OK;
+  });
+}

@@ -19,12 +19,13 @@ PHX_OK, PHX_E_INVALID, PHX_E_IO, PHX_E_CUDA, PHX_E_TIMEOUT, PHX_E_UNSUPPORTED = 
 PREC_FP32, PREC_FP64, PREC_MIXED = 0, 1, 2
 PRECISIONS = {"fp32": PREC_FP32, "fp64": PREC_FP64, "mixed": PREC_MIXED}
 SNAP_F64_PRIMS = 1
+NOALLOC_MAX_JOBS = 1 << 20
 NUM_COUNTERS = 16
 CTR = dict(queue=0, steps=1, nplasma=2, bad=3, scans=4, fp64_steps=5, fp64_ops=6, rays=7)
 
 # Every symbol include/phoenix_b200.h declares.
 EXPORTS = ["phx_default_params", "phx_snapshot_create", "phx_snapshot_load", "phx_snapshot_destroy",
-           "phx_bhac_read", "phx_bhac_describe", "phx_bhac_free", "phx_snapshot_bytes", "phx_schedule_morton", "phx_render", "phx_render_async", "phx_last_error",
+           "phx_bhac_read", "phx_bhac_describe", "phx_bhac_free", "phx_snapshot_bytes", "phx_schedule_morton", "phx_render", "phx_render_async", "phx_render_noalloc", "phx_last_error",
            "phx_version"]
 
 
@@ -109,10 +110,11 @@ def lib():
     L.phx_render.argtypes = [C.c_void_p, P(PhxRenderParams), C.c_void_p, C.c_int64, C.c_void_p, P(PhxRenderInfo)]
     L.phx_render_async.argtypes = [C.c_void_p, P(PhxRenderParams), C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p]
+    L.phx_render_noalloc.argtypes = [C.c_void_p, P(PhxRenderParams), C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
     L.phx_last_error.restype = C.c_char_p
     L.phx_version.restype = C.c_char_p
     for name in ("phx_snapshot_create", "phx_snapshot_load", "phx_bhac_read", "phx_bhac_describe", "phx_schedule_morton",
-                 "phx_render", "phx_render_async"):
+                 "phx_render", "phx_render_async", "phx_render_noalloc"):
         getattr(L, name).restype = C.c_int
     _lib = L
     return L
