@@ -33,7 +33,8 @@ LIB = os.path.join(BUILD, "libphoenix_b200.so")
 CLI = os.path.join(BUILD, "PHOENIX")
 GEN = os.path.join(BUILD, "phx_gen_snapshot")
 
-DEVICE_SRC = ["device/march_fp32.cu", "device/march_mixed.cu", "device/march_fp64.cu", "device/capi.cu"]
+DEVICE_SRC = ["device/march_fp64_f64.cu", "device/march_fp64_f32.cu", "device/march_fp32_nf1.cu", "device/march_fp32_nf4.cu",
+              "device/march_mixed_nf1.cu", "device/march_mixed_nf4.cu", "device/march_dispatch.cu", "device/capi.cu"]
 HOST_SRC = ["host/snapshot.cpp"]
 CLI_SRC = ["host/main.cpp", "host/config.cpp", "host/output.cpp"]
 

@@ -44,8 +44,10 @@ template <class T>
 PHX_HD KerrPt<T> kerr_point(T a, T hs, T x1, T x2) {
   KerrPt<T> p;
   p.r = exp_t(x1);
-  T s2x, c2x;
-  sincos_t(T(2) * x2, &s2x, &c2x);
+  // sin 2x2, cos 2x2 from one sincos of x2 (double-angle identities)
+  T sx, cx;
+  sincos_t(x2, &sx, &cx);
+  const T s2x = T(2) * sx * cx, c2x = (cx - sx) * (cx + sx);
   const T th = x2 + T(0.5) * hs * s2x;
   p.tp = T(1) + hs * c2x;
   p.tpp = T(-2) * hs * s2x;

@@ -106,7 +106,11 @@ struct Ray {
     }
     const R r = exp_t(cx[1]);
     const bool alive = r < rc.r_out && r > rc.cut_in && steps < rc.max_steps && !terminate;
-    const bool need_leaf = pvalid && alive;
+    // The pending sample's plasma stage only runs inside rt_outer (the reference samples the fluid further out too,
+    // but always discards it there: derive_fluid and process_sample both require r < rt_outer, and the sampler cache
+    // the lookup seeds is local to that sample), so its cache seed is only needed then.
+    const bool pend_plasma = pvalid && exp_t(px[1]) < rc.rt_outer;
+    const bool need_leaf = pend_plasma && alive;
     const bool need_dxc = alive && r < rc.rt_outer;
     int L = -1;
     R xw[4] = {cx[0], cx[1], cx[2], cx[3]};
@@ -116,7 +120,7 @@ struct Ray {
       L = find_leaf(s, xw, &scanned);
       ctr.scans += scanned;
     }
-    if (pvalid) {
+    if (pend_plasma) {
       int right = -1;
       if (need_leaf) right = (exp_t(xw[1]) < R(1) || outside_domain(s, xw)) ? -1 : L;
       process_sample(s, rc, right, ctr);

@@ -120,6 +120,11 @@ struct LaunchShape {
   int block, grid, regs, local_bytes, blocks_per_sm;
 };
 
+// One frequency-slot instantiation (defined in march_impl.cuh, instantiated by the march_*.cu files).
+template <Mode M, class PT, int NF>
+cudaError_t launch_nf(const MarchArgs<typename Policy<M>::R, PT>& args, int sms, int blocks_per_sm,
+                      cudaStream_t stream, LaunchShape* shape);
+
 template <Mode M, class PT>
 cudaError_t launch_march(const MarchArgs<typename Policy<M>::R, PT>& args, int sms, int blocks_per_sm,
                          cudaStream_t stream, LaunchShape* shape);

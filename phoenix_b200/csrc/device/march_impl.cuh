@@ -1,27 +1,23 @@
-// Launch logic of the raymarch kernel (see march.cuh); each march_<mode>.cu instantiates it for one mode.
+// Launch logic of the raymarch kernel (see march.cuh); each march_<mode>_nf<slots>.cu file instantiates launch_nf.
 #pragma once
 
 #include "march.cuh"
 
 namespace phx {
 
-namespace {
-
 constexpr int kBlock = 128;
 
-template <Mode M, class PT, int NF>
-cudaError_t launch_nf(const MarchArgs<typename Policy<M>::R, PT>& args, int sms, int blocks_per_sm,
-                      cudaStream_t stream, LaunchShape* shape) {
-  auto kern = k_march<M, PT, NF, kBlock, 1>;
+template <Mode M, class PT, int NF, int kMinBlocks>
+cudaError_t launch_mb(const MarchArgs<typename Policy<M>::R, PT>& args, int sms, cudaStream_t stream,
+                      LaunchShape* shape) {
+  auto kern = k_march<M, PT, NF, kBlock, kMinBlocks>;
   cudaFuncAttributes fa;
   cudaError_t e = cudaFuncGetAttributes(&fa, kern);
   if (e != cudaSuccess) return e;
-  int bpsm = blocks_per_sm;
-  if (bpsm <= 0) {
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, kern, kBlock, 0);
-    if (e != cudaSuccess) return e;
-    if (bpsm < 1) bpsm = 1;
-  }
+  int bpsm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, kern, kBlock, 0);
+  if (e != cudaSuccess) return e;
+  if (bpsm < 1) bpsm = 1;
   long long grid = (long long)bpsm * sms;
   const long long need = (args.njobs + kBlock - 1) / kBlock;
   if (grid > need) grid = need;
@@ -36,15 +32,29 @@ cudaError_t launch_nf(const MarchArgs<typename Policy<M>::R, PT>& args, int sms,
   return cudaGetLastError();
 }
 
-}  // namespace
-
-template <Mode M, class PT>
-cudaError_t launch_march(const MarchArgs<typename Policy<M>::R, PT>& args, int sms, int blocks_per_sm,
-                         cudaStream_t stream, LaunchShape* shape) {
-  const int nf = args.rc.nfreqs;
-  if (nf <= 1) return launch_nf<M, PT, 1>(args, sms, blocks_per_sm, stream, shape);
-  if (nf <= 4) return launch_nf<M, PT, 4>(args, sms, blocks_per_sm, stream, shape);
-  return launch_nf<M, PT, kMaxFreqs>(args, sms, blocks_per_sm, stream, shape);
+// Register-cap variants: `blocks_per_sm` picks the instantiation compiled for that many resident 128-thread blocks
+// per SM (__launch_bounds__ min blocks: 1 -> up to 255 registers, 3 -> 168, 4 -> 128; 0 = default).  FP64 and the 32-slot
+// variants are compiled uncapped only.
+template <Mode M, class PT, int NF>
+cudaError_t launch_nf(const MarchArgs<typename Policy<M>::R, PT>& args, int sms, int blocks_per_sm,
+                      cudaStream_t stream, LaunchShape* shape) {
+  if constexpr (M == Mode::kFP64 || NF > 4) {
+    (void)blocks_per_sm;
+    return launch_mb<M, PT, NF, 1>(args, sms, stream, shape);
+  } else {
+    switch (blocks_per_sm) {
+      case 1:
+      case 2:
+        return launch_mb<M, PT, NF, 1>(args, sms, stream, shape);
+      case 3:
+        return launch_mb<M, PT, NF, 3>(args, sms, stream, shape);
+      case 4:
+        return launch_mb<M, PT, NF, 4>(args, sms, stream, shape);
+      default:  // measured on B200: 4 resident blocks (128 registers) for one slot, 3 for four
+        if constexpr (NF == 1) return launch_mb<M, PT, NF, 4>(args, sms, stream, shape);
+        else return launch_mb<M, PT, NF, 3>(args, sms, stream, shape);
+    }
+  }
 }
 
 }  // namespace phx

@@ -26,10 +26,101 @@
 #include <string>
 #include <vector>
 
-#include "../core/decode.cuh"
+#include "../core/defs.cuh"
 #include "../host/bhac_format.hpp"
 
 namespace {
+
+// The generator keeps its own FP64 metric arithmetic (rather than the render headers, which are tuned for the
+// kernel) so that the bytes it writes for a given seed never change.
+namespace gm {
+
+struct Pt {
+  double r, s, c, s2, tp, sig, q;
+};
+
+Pt point(double a, double hs, double x1, double x2) {
+  Pt p;
+  p.r = std::exp(x1);
+  const double s2x = std::sin(2.0 * x2), c2x = std::cos(2.0 * x2);
+  const double th = x2 + 0.5 * hs * s2x;
+  p.tp = 1.0 + hs * c2x;
+  p.s = std::sin(th);
+  p.c = std::cos(th);
+  p.s2 = p.s * p.s;
+  p.sig = p.r * p.r + a * a * p.c * p.c;
+  p.q = 2.0 * p.r / p.sig;
+  return p;
+}
+
+struct Cov {
+  double tt, t1, t3, x11, x13, x22, x33;
+};
+
+Cov cov(const Pt& p, double a) {
+  Cov g;
+  const double opq = 1.0 + p.q;
+  g.tt = p.q - 1.0;
+  g.t1 = p.q * p.r;
+  g.t3 = -a * p.s2 * p.q;
+  g.x11 = opq * p.r * p.r;
+  g.x13 = -a * p.s2 * opq * p.r;
+  g.x22 = p.sig * p.tp * p.tp;
+  g.x33 = p.s2 * (p.sig + a * a * p.s2 * opq);
+  return g;
+}
+
+struct Contra {
+  double tt, t1;
+};
+
+Contra contra(const Pt& p) {
+  Contra u;
+  u.tt = -(1.0 + p.q);
+  u.t1 = 2.0 / p.sig;
+  return u;
+}
+
+// out = g V over the spatial block (V^0 = 0) plus the g_t. column (used for lowering spatial vectors).
+void lower(const Cov& g, const double V[4], double out[4]) {
+  out[0] = g.tt * V[0] + g.t1 * V[1] + g.t3 * V[3];
+  out[1] = g.t1 * V[0] + g.x11 * V[1] + g.x13 * V[3];
+  out[2] = g.x22 * V[2];
+  out[3] = g.t3 * V[0] + g.x13 * V[1] + g.x33 * V[3];
+}
+
+double sqrt_det_gamma(double a, double hs, double x1, double x2) {
+  const Cov g = cov(point(a, hs, x1, x2), a);
+  return std::sqrt(g.x22 * (g.x11 * g.x33 - g.x13 * g.x13));
+}
+
+// Volume-weighted cell centroid (Simpson 1-4-1 per axis), the point every BHAC reader evaluates the metric at.
+void centroid(double a, double hs, const double X[3], const double dx[3], double Xbar[3]) {
+  const double w1[3] = {1.0, 4.0, 1.0};
+  double norm = 0.0, s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (int k = 0; k < 3; k++) {
+    const double z = X[2] + 0.5 * dx[2] * (k - 1);
+    for (int j = 0; j < 3; j++) {
+      const double y = X[1] + 0.5 * dx[1] * (j - 1);
+      for (int i = 0; i < 3; i++) {
+        const double x = X[0] + 0.5 * dx[0] * (i - 1);
+        const double w = w1[i] * w1[j] * w1[k] * sqrt_det_gamma(a, hs, x, y);
+        norm += w;
+        s0 += w * x;
+        s1 += w * y;
+        s2 += w * z;
+      }
+    }
+  }
+  Xbar[0] = s0 / norm;
+  Xbar[1] = s1 / norm;
+  Xbar[2] = s2 / norm;
+}
+
+}  // namespace gm
+
+// Conserved slots of the dump (D, S_1..3, tau, B^1..3, D s, then Lorentz factor and xi).
+enum { kCD = 0, kCS1 = 1, kCTau = 4, kCB1 = 5, kCDS = 8 };
 
 struct Opts {
   std::string out = ".";
@@ -128,7 +219,7 @@ struct Gen {
         psum += K * std::pow(rt, o.gam);
         double B1, B2;
         field(x1, x2, &B1, &B2);
-        phx::Cov<double> g = phx::cov_metric(phx::kerr_point(o.spin, o.hslope, x1, x2), o.spin);
+        const gm::Cov g = gm::cov(gm::point(o.spin, o.hslope, x1, x2), o.spin);
         bsum += 0.5 * (g.x11 * B1 * B1 + g.x22 * B2 * B2);
       }
     }
@@ -200,10 +291,10 @@ struct Gen {
 
       // metric at the centroid (the decode uses the same point)
       double Xb[3];
-      phx::cell_centroid(a, o.hslope, X, dx, Xb);
-      const phx::KerrPt<double> p = phx::kerr_point(a, o.hslope, Xb[0], Xb[1]);
-      const phx::Cov<double> g = phx::cov_metric(p, a);
-      const phx::Contra<double> gu = phx::contra_metric(p, a);
+      gm::centroid(a, o.hslope, X, dx, Xb);
+      const gm::Pt p = gm::point(a, o.hslope, Xb[0], Xb[1]);
+      const gm::Cov g = gm::cov(p, a);
+      const gm::Contra gu = gm::contra(p);
       const double alpha = 1.0 / std::sqrt(-gu.tt);
       const double beta1 = gu.t1 / (-gu.tt);  // shift (beta^2 = beta^3 = 0)
 
@@ -220,18 +311,18 @@ struct Gen {
         }
       }
       double gvd[4];
-      phx::symv(g, gv, gvd);
+      gm::lower(g, gv, gvd);
       const double mag = std::sqrt(std::max(gvd[1] * gv[1] + gvd[2] * gv[2] + gvd[3] * gv[3], 0.0));
       for (int d = 1; d <= 3; d++) gv[d] += o.vpert * mag * gauss(key, d);
-      phx::symv(g, gv, gvd);
+      gm::lower(g, gv, gvd);
       const double lfac = std::sqrt(1.0 + gvd[1] * gv[1] + gvd[2] * gv[2] + gvd[3] * gv[3]);
       (void)alpha;
 
       // conserved variables
       const double v[4] = {0.0, gv[1] / lfac, gv[2] / lfac, gv[3] / lfac};
       double vd[4], Bd[4];
-      phx::symv(g, v, vd);
-      phx::symv(g, B, Bd);
+      gm::lower(g, v, vd);
+      gm::lower(g, B, Bd);
       const double Bsq = Bd[1] * B[1] + Bd[2] * B[2] + Bd[3] * B[3];
       const double Bv = Bd[1] * v[1] + Bd[2] * v[2] + Bd[3] * v[3];
       const double v2 = vd[1] * v[1] + vd[2] * v[2] + vd[3] * v[3];
@@ -239,11 +330,11 @@ struct Gen {
       const double press = (gam - 1.0) * uu;
       const double D = rho * lfac;
       double* c = out;
-      c[(size_t)phx::kCD * cells + cell] = D;
-      for (int d = 1; d <= 3; d++) c[(size_t)(phx::kCS1 + d - 1) * cells + cell] = (xi + Bsq) * vd[d] - Bv * Bd[d];
-      c[(size_t)phx::kCTau * cells + cell] = xi - press - D + 0.5 * (Bsq + Bsq * v2 - Bv * Bv);
-      for (int d = 1; d <= 3; d++) c[(size_t)(phx::kCB1 + d - 1) * cells + cell] = B[d];
-      c[(size_t)phx::kCDS * cells + cell] = D * press / std::pow(rho, gam);
+      c[(size_t)kCD * cells + cell] = D;
+      for (int d = 1; d <= 3; d++) c[(size_t)(kCS1 + d - 1) * cells + cell] = (xi + Bsq) * vd[d] - Bv * Bd[d];
+      c[(size_t)kCTau * cells + cell] = xi - press - D + 0.5 * (Bsq + Bsq * v2 - Bv * Bv);
+      for (int d = 1; d <= 3; d++) c[(size_t)(kCB1 + d - 1) * cells + cell] = B[d];
+      c[(size_t)kCDS * cells + cell] = D * press / std::pow(rho, gam);
       c[(size_t)9 * cells + cell] = lfac;
       c[(size_t)10 * cells + cell] = xi;
     }
