@@ -170,6 +170,14 @@ int phx_render_async(PhxSnapshot* s, const PhxRenderParams* p, const int32_t* d_
 int phx_render_noalloc(PhxSnapshot* s, const PhxRenderParams* p, const int32_t* jobs, int64_t njobs,
                        PhxFreqOut* d_res, void* stream);
 
+/* Writes a render's outputs the way PHOENIX's write_output does (src/main.cpp:52-86, src/host/io/output.hpp):
+ * `image` = "hdf5" -> outdir/img_data.h5 (RAPTOR block layout, block_size pixels per side; if it cannot be written the
+ * text image is written instead), "text" -> outdir/image.dat (image_<f>.dat per frequency when nfreqs > 1),
+ * "both", or "none"; always outdir/spectrum.dat.  flux (NULL or nfreqs x 4) receives the total I, Q, U, V [Jy]
+ * per frequency.  The directory must exist. */
+int phx_write_output(const PhxRenderParams* p, const PhxFreqOut* res, const char* outdir, const char* image,
+                     int32_t block_size, double* flux);
+
 /* Description of the last error on this host thread. */
 const char* phx_last_error(void);
 

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "../../../include/phoenix_b200.h"
+#include "../host/output.hpp"
 #include "../host/render_setup.hpp"
 #include "../host/snapshot.hpp"
 #include "march.cuh"
@@ -439,6 +440,33 @@ int phx_render(PhxSnapshot* s, const PhxRenderParams* p, const int32_t* jobs, in
       info->fp64_steps = (int64_t)ctr[phx::kCtrFp64Steps];
       info->fp64_ops = (int64_t)ctr[phx::kCtrFp64Ops];
     }
+    return PHX_OK;
+  });
+}
+
+int phx_write_output(const PhxRenderParams* p, const PhxFreqOut* res, const char* outdir, const char* image,
+                     int32_t block_size, double* flux) {
+  return guarded([&]() -> int {
+    if (!p || !res || !outdir || !image) throw std::invalid_argument("null argument");
+    if (p->img_width < 1 || p->img_height < 1 || p->nfreqs < 1 || p->nfreqs > PHX_MAX_FREQS)
+      throw std::invalid_argument("bad image size or frequency count");
+    const std::string mode = image, dir = outdir;
+    if (mode != "hdf5" && mode != "text" && mode != "both" && mode != "none")
+      throw std::invalid_argument("image must be hdf5, text, both or none");
+    const std::vector<PhxFreqOut> r(res, res + (size_t)p->img_width * p->img_height * p->nfreqs);
+    bool want_text = mode == "text" || mode == "both";
+    if (mode == "hdf5" || mode == "both") {
+      std::string err;
+      if (!phx::write_image_hdf5(dir + "/img_data.h5", *p, block_size, r, &err)) want_text = true;
+    }
+    if (want_text)
+      for (int f = 0; f < p->nfreqs; f++) {
+        const std::string ip = dir + "/image" + (p->nfreqs == 1 ? "" : "_" + std::to_string(f)) + ".dat";
+        if (!phx::write_image_text(ip, *p, r, f)) throw std::runtime_error("cannot write " + ip);
+      }
+    if (!phx::write_spectrum(dir + "/spectrum.dat", *p, r)) throw std::runtime_error("cannot write spectrum.dat");
+    if (flux)
+      for (int f = 0; f < p->nfreqs; f++) phx::compute_spec(*p, r, f, flux + 4 * f);
     return PHX_OK;
   });
 }

@@ -25,7 +25,7 @@ CTR = dict(queue=0, steps=1, nplasma=2, bad=3, scans=4, fp64_steps=5, fp64_ops=6
 
 # Every symbol include/phoenix_b200.h declares.
 EXPORTS = ["phx_default_params", "phx_snapshot_create", "phx_snapshot_load", "phx_snapshot_destroy",
-           "phx_bhac_read", "phx_bhac_describe", "phx_bhac_free", "phx_snapshot_bytes", "phx_schedule_morton", "phx_render", "phx_render_async", "phx_render_noalloc", "phx_last_error",
+           "phx_bhac_read", "phx_bhac_describe", "phx_bhac_free", "phx_snapshot_bytes", "phx_schedule_morton", "phx_render", "phx_render_async", "phx_render_noalloc", "phx_write_output", "phx_last_error",
            "phx_version"]
 
 
@@ -111,6 +111,8 @@ def lib():
     L.phx_render_async.argtypes = [C.c_void_p, P(PhxRenderParams), C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p]
     L.phx_render_noalloc.argtypes = [C.c_void_p, P(PhxRenderParams), C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
+    L.phx_write_output.argtypes = [P(PhxRenderParams), C.c_void_p, C.c_char_p, C.c_char_p, C.c_int32, C.c_void_p]
+    L.phx_write_output.restype = C.c_int
     L.phx_last_error.restype = C.c_char_p
     L.phx_version.restype = C.c_char_p
     for name in ("phx_snapshot_create", "phx_snapshot_load", "phx_bhac_read", "phx_bhac_describe", "phx_schedule_morton",
@@ -153,3 +155,14 @@ def schedule_morton(width: int, height: int) -> np.ndarray:
     jobs = np.empty(width * height, dtype=np.int32)
     check(lib().phx_schedule_morton(width, height, jobs.ctypes.data))
     return jobs
+
+
+def write_output(res, params, outdir: str, image: str = "hdf5", block_size: int = 10):
+    """Write img_data.h5 / image*.dat / spectrum.dat like PHOENIX; returns the flux [nfreqs, 4] in Jy."""
+    r = np.ascontiguousarray(res, dtype=np.float64)
+    if r.size != params.img_width * params.img_height * params.nfreqs * 6:
+        raise ValueError("res does not match the image size")
+    flux = np.zeros((params.nfreqs, 4))
+    check(lib().phx_write_output(C.byref(params), r.ctypes.data, outdir.encode(), image.encode(), block_size,
+                                 flux.ctypes.data))
+    return flux
