@@ -129,13 +129,19 @@ def test_frequencies_are_independent(gpu_snapshots):
         assert np.abs(multi[:, :, f] - single[:, :, 0]).max() <= 1e-12 * scale
 
 
-@pytest.mark.parametrize("period,bps", [(1, 0), (4, 1), (16, 0)])
-def test_results_independent_of_launch_shape(gpu_snapshots, period, bps):
-    """Each ray's arithmetic does not depend on which lane or warp runs it: bit-identical images."""
+@pytest.mark.parametrize("bps", [0, 1, 3])
+def test_results_independent_of_scheduling(gpu_snapshots, bps):
+    """A ray's arithmetic does not depend on which lane, warp or refill round runs it: for one compiled variant the
+    image is bit-identical whatever the refill period.  Variants compiled for other register caps round differently
+    (separate compilations), so across them the images agree to FP32 rounding."""
     kw = case_params("cfg1")
-    base, _ = gpu_snapshots["cfg1"].render(P.make_params(precision="fp32", **kw))
-    other, _ = gpu_snapshots["cfg1"].render(P.make_params(precision="fp32", period=period, blocks_per_sm=bps, **kw))
-    assert np.array_equal(base, other)
+    base, _ = gpu_snapshots["cfg1"].render(P.make_params(precision="fp32", blocks_per_sm=bps, period=1, **kw))
+    for period in (4, 16, 64):
+        other, _ = gpu_snapshots["cfg1"].render(P.make_params(precision="fp32", blocks_per_sm=bps, period=period, **kw))
+        assert np.array_equal(base, other), (bps, period)
+    default, _ = gpu_snapshots["cfg1"].render(P.make_params(precision="fp32", **kw))
+    l1 = np.abs(default[..., :4] - base[..., :4]).sum() / np.abs(base[..., :4]).sum()
+    assert l1 <= 1e-5, l1
 
 
 def test_invalid_arguments_are_reported(gpu_snapshots):
