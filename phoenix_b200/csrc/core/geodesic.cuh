@@ -59,7 +59,9 @@ PHX_HD R pole_x2(const GeoState<R>& g) {
 }
 
 // One classical RK4 step of length dt.  Stage sums are kept as (d0 + d3) and (d1 + d2) so that the update
-// ((d0 + d3) + 2 (d1 + d2)) dt/6 needs two 12-vectors instead of four.
+// ((d0 + d3) + 2 (d1 + d2)) dt/6 needs two 12-vectors instead of four.  The stage loop is deliberately not unrolled:
+// one copy of the stage body (metric, derivatives, both Christoffel contractions) keeps the march loop small enough
+// for the instruction cache, which four unrolled copies overflow.
 template <class R, bool kComp>
 PHX_HD void rk4_step(R a, R hs, GeoState<R>& g, R dt) {
   const R pi_hi = R(kPi), pi_lo = R(kPi - (double)R(kPi));
@@ -67,7 +69,7 @@ PHX_HD void rk4_step(R a, R hs, GeoState<R>& g, R dt) {
   R inc[12], s03[12], s12[12];
 #pragma unroll
   for (int i = 0; i < 12; i++) inc[i] = R(0);
-#pragma unroll
+#pragma unroll 1
   for (int q = 0; q < 4; q++) {
     R y[12];
 #pragma unroll

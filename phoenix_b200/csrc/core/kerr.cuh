@@ -24,8 +24,9 @@ struct KerrPt {
   T s2;   // sin^2(theta)
   T tp;   // d theta / d x2
   T tpp;  // d^2 theta / d x2^2
-  T sig;  // Sigma = r^2 + a^2 cos^2(theta)
-  T q;    // 2 r / Sigma
+  T sig;   // Sigma = r^2 + a^2 cos^2(theta)
+  T isig;  // 1 / Sigma
+  T q;     // 2 r / Sigma
 };
 
 // Non-zero covariant components g_{mu nu} (symmetric).
@@ -54,7 +55,8 @@ PHX_HD KerrPt<T> kerr_point(T a, T hs, T x1, T x2) {
   sincos_t(th, &p.s, &p.c);
   p.s2 = p.s * p.s;
   p.sig = p.r * p.r + a * a * p.c * p.c;
-  p.q = T(2) * p.r / p.sig;
+  p.isig = T(1) / p.sig;
+  p.q = T(2) * p.r * p.isig;
   return p;
 }
 
@@ -75,14 +77,16 @@ PHX_HD Cov<T> cov_metric(const KerrPt<T>& p, T a) {
 template <class T>
 PHX_HD Contra<T> contra_metric(const KerrPt<T>& p, T a) {
   Contra<T> u;
-  const T isig = T(1) / p.sig;
+  const T isig = p.isig;
   const T ir = T(1) / p.r;
+  const T tp2 = p.tp * p.tp;
+  const T iprod = isig / (tp2 * p.s2);  // one division for both 1 / theta'^2 and 1 / sin^2
   u.tt = -(T(1) + p.q);
   u.t1 = T(2) * isig;
   u.x11 = isig * ((p.r - T(2)) * p.r + a * a) * ir * ir;
   u.x13 = a * isig * ir;
-  u.x22 = isig / (p.tp * p.tp);
-  u.x33 = isig / p.s2;
+  u.x22 = iprod * p.s2;
+  u.x33 = iprod * tp2;
   return u;
 }
 
@@ -145,7 +149,7 @@ template <class T>
 PHX_HD void cov_derivs(const KerrPt<T>& p, T a, Cov<T>* D1, Cov<T>* D2) {
   const T a2 = a * a, r = p.r, r2 = r * r, q = p.q, opq = T(1) + q;
   // x1: dr/dx1 = r, dSigma/dx1 = 2 r^2, dq/dx1 = q (1 - 2 r^2 / Sigma)
-  const T q1 = q * (T(1) - T(2) * r2 / p.sig);
+  const T q1 = q * (T(1) - T(2) * r2 * p.isig);
   D1->tt = q1;
   D1->t1 = (q1 + q) * r;
   D1->t3 = -a * p.s2 * q1;
@@ -156,7 +160,7 @@ PHX_HD void cov_derivs(const KerrPt<T>& p, T a, Cov<T>* D1, Cov<T>* D2) {
   // x2: d(sin^2)/dx2 = 2 s c theta', dSigma/dx2 = -2 a^2 s c theta', dq/dx2 = -q dSigma / Sigma
   const T sc2 = T(2) * p.s * p.c * p.tp;
   const T sig2 = -a2 * sc2;
-  const T q2 = -q * sig2 / p.sig;
+  const T q2 = -q * sig2 * p.isig;
   D2->tt = q2;
   D2->t1 = q2 * r;
   D2->t3 = -a * (sc2 * q + p.s2 * q2);

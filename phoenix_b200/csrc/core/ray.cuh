@@ -10,10 +10,15 @@
 //   FP32   float everywhere after the FP64 camera set-up; compensated (hi, lo) geodesic state with south-pole
 //          folding; deviation-form transfer operator.
 //   FP64   double everywhere.
-//   Mixed  FP32 bulk plus four FP64 islands: RK4 steps inside r < r_fp64 (default 1.5 r_horizon), the null-condition
+//   Mixed  FP32 bulk plus FP64 islands: RK4 steps inside r < r_fp64 (default 1.5 r_horizon), the null-condition
 //          renormalisation of each sample's wave vector, the segment operator where h max|K| > tau_fp64 (large
-//          optical / Faraday depth per segment), and Kahan summation of the Stokes vector.
+//          optical / Faraday depth per segment), Kahan summation of the Stokes vector, and the placement of samples
+//          in leaves and cells (the compensated FP32 position widened to FP64 against FP64 leaf geometry).  The last
+//          island removes the dominant FP32 error: the reference's interpolation is block-local, so a sample that FP32
+//          rounding moves across a block face picks up the neighbour block's values.
 #pragma once
+
+#include <type_traits>
 
 #include "camera.cuh"
 #include "defs.cuh"
@@ -71,6 +76,7 @@ struct Ray {
 
   GeoState<R> geo;
   R px[4], pk[4], pF[4], pdl;
+  std::conditional_t<kMixed, double, char> pxd[4];  // mixed: the pending sample's compensated position in FP64
   bool pvalid, terminate;
   int steps, turns, bsign, nplasma, bad;
   R thdot_prev, dl_prev;
@@ -112,24 +118,23 @@ struct Ray {
     const bool pend_plasma = pvalid && exp_t(px[1]) < rc.rt_outer;
     const bool need_leaf = pend_plasma && alive;
     const bool need_dxc = alive && r < rc.rt_outer;
-    int L = -1;
-    R xw[4] = {cx[0], cx[1], cx[2], cx[3]};
+    int L = -1, right = -1;
     if (need_leaf || need_dxc) {
+      // the step-size cap and the sample's cache seed: FP32 in every FP32 mode (mixed re-checks the seed in FP64)
+      R xw[4] = {cx[0], cx[1], cx[2], cx[3]};
       wrap_coords(xw);
       bool scanned = false;
       L = find_leaf(s, xw, &scanned);
       ctr.scans += scanned;
-    }
-    if (pend_plasma) {
-      int right = -1;
       if (need_leaf) right = (exp_t(xw[1]) < R(1) || outside_domain(s, xw)) ? -1 : L;
-      process_sample(s, rc, right, ctr);
     }
+    if (pend_plasma) process_sample(s, rc, right, ctr);
 #pragma unroll
     for (int i = 0; i < 4; i++) {
       px[i] = cx[i];
       pk[i] = ck[i];
       pF[i] = cF[i];
+      if constexpr (kMixed) pxd[i] = (double)geo.hi[i] + (double)geo.lo[i];
     }
     pdl = dl_prev;
     pvalid = steps >= 1;
@@ -183,37 +188,58 @@ struct Ray {
     }
     // sampler (sampler.hpp:387-427): wrap, domain, cached leaf or a fresh lookup of the re-wrapped point
     R x[4] = {px[0], px[1], px[2], px[3]};
-    wrap_coords(x);
-    if (exp_t(x[1]) < R(1)) return;
-    if (outside_domain(s, x)) return;
     int ig = right;
-    if (ig == -1 || !inside_cached(s, ig, x)) {
-      wrap_coords(x);
-      bool scanned = false;
-      ig = find_leaf(s, x, &scanned);
-      ctr.scans += scanned;
-    }
-    if (ig == -1) return;
     R q[kNPrim];
-    interp_prims<R, PT, !kComp>(s, ig, x, q);
+    if constexpr (kMixed) {
+      double xd[4] = {pxd[0], pxd[1], pxd[2], pxd[3]};
+      const SnapView<double, PT> sd = s.fp64_view();
+      wrap_coords(xd);
+      if (exp_t(xd[1]) < 1.0) return;
+      if (outside_domain(sd, xd)) return;
+      if (ig == -1 || !inside_cached(sd, ig, xd)) {
+        wrap_coords(xd);
+        bool scanned = false;
+        ig = find_leaf(sd, xd, &scanned);
+        ctr.scans += scanned;
+      }
+      if (ig == -1) return;
+      double qd[kNPrim];
+      interp_prims<double, PT, true>(sd, ig, xd, qd);
+#pragma unroll
+      for (int v = 0; v < kNPrim; v++) q[v] = R(qd[v]);
+#pragma unroll
+      for (int i = 0; i < 4; i++) x[i] = R(xd[i]);
+    } else {
+      wrap_coords(x);
+      if (exp_t(x[1]) < R(1)) return;
+      if (outside_domain(s, x)) return;
+      if (ig == -1 || !inside_cached(s, ig, x)) {
+        wrap_coords(x);
+        bool scanned = false;
+        ig = find_leaf(s, x, &scanned);
+        ctr.scans += scanned;
+      }
+      if (ig == -1) return;
+      interp_prims<R, PT, !kComp>(s, ig, x, q);
+    }
     const KerrPt<R> p = kerr_point(s.a, s.hs, x[1], x[2]);
     const Cov<R> g = cov_metric(p, s.a);
     const Contra<R> u = contra_metric(p, s.a);
     Fluid<R> fl;
     if (!derive_fluid(rc.pv, s.gam, exp_t(x[1]), g, u, q, &fl)) return;
     if (!(r < rc.rt_outer)) return;
-    // pitch angle of k to B in the plasma frame (tetrad.hpp:138-154)
+    // pitch angle of k to B in the plasma frame (tetrad.hpp:138-154): only its sine and cosine enter the
+    // coefficients, so they are formed from mu = cos(pitch) directly; acos(mu) is 0 or pi exactly when mu = +-1
     const R Bn = sqrt_t(fabs_t(dot(g, fl.B, fl.B)));
     const R kU = dot(g, k, fl.U);
-    R pitch;
-    if (Bn == R(0)) {
-      pitch = R(kHalfPi);
-    } else {
+    R sth = R(1), cth = R(0);
+    if (Bn != R(0)) {
       R mu = dot(g, k, fl.B) / (fabs_t(kU) * Bn);
       if (fabs_t(mu) > R(1)) mu /= fabs_t(mu);
-      pitch = acos_t(mu);
+      if (mu == R(1) || mu == R(-1)) return;
+      sth = sqrt_t((R(1) - mu) * (R(1) + mu));
+      cth = mu;
     }
-    if (pitch == R(0) || pitch == R(kPi)) return;
     // polarization axes of the plasma frame with B as reference direction; EVPA rotation from the transported F1
     R perp[4], para[4], omega;
     observer_axes(g, sqrt_neg_g(p), k, fl.U, fl.B, perp, para, &omega);
@@ -221,7 +247,7 @@ struct Ray {
     const R nn = C * C + S * S;
     const R c2 = (C * C - S * S) / nn, s2 = R(2) * C * S / nn;
     const R ratio = -kU;  // nu_plasma / nu_camera
-    const SynchroSample<R> ss = synchro_sample(fl.theta_e, fl.n_e, fl.Bmag, pitch);
+    const SynchroSample<R> ss = synchro_sample(fl.theta_e, fl.n_e, fl.Bmag, sth, cth);
 #pragma unroll
     for (int f = 0; f < NF; f++) {
       if (f >= rc.nfreqs) break;

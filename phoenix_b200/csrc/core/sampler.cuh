@@ -31,6 +31,36 @@ struct SnapView {
   R x_lo[4], x_hi[4];
   R w0[3];  // base-level block widths
   R a, hs, gam;
+  // FP64 leaf geometry, used by the mixed-precision path to place FP32 samples in leaves and cells exactly
+  const double* lbd;
+  const double* dxcd;
+  double xlo_d[4], xhi_d[4], w0_d[3];
+
+  PHX_HD SnapView<double, PT> fp64_view() const {
+    SnapView<double, PT> v;
+    v.lb = lbd;
+    v.dxc = dxcd;
+    v.prim = prim;
+    v.fmap = fmap;
+    for (int d = 0; d < 3; d++) {
+      v.fd[d] = fd[d];
+      v.nx[d] = nx[d];
+      v.w0[d] = w0_d[d];
+    }
+    for (int d = 0; d < 4; d++) {
+      v.x_lo[d] = xlo_d[d];
+      v.x_hi[d] = xhi_d[d];
+    }
+    v.nleafs = nleafs;
+    v.nlevels = nlevels;
+    v.cells = cells;
+    v.a = a;
+    v.hs = hs;
+    v.gam = gam;
+    v.lbd = lbd;
+    v.dxcd = dxcd;
+    return v;
+  }
 };
 
 // Per-render plasma constants.

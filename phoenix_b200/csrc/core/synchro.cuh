@@ -101,17 +101,19 @@ struct SynchroSample {
   R omega0;        // gyro frequency
 };
 
+// sth, cth: sine and cosine of the pitch angle (computed from its cosine directly; no angle is formed).
 template <class R>
-PHX_HD SynchroSample<R> synchro_sample(R te, R ne, R B, R thB) {
+PHX_HD SynchroSample<R> synchro_sample(R te, R ne, R B, R sth, R cth) {
   constexpr double NU_CRIT = 3.0 * cgs::q_electron / (4.0 * kPi * cgs::m_electron * cgs::c_light);
   constexpr double JNU = cgs::q_electron * cgs::q_electron / (2.0 * 1.73205080756887729353 * cgs::c_light);
   constexpr double WP2 = 4.0 * kPi * cgs::q_electron * cgs::q_electron / cgs::m_electron;
   constexpr double GYRO = cgs::q_electron / (cgs::m_electron * cgs::c_light);
   SynchroSample<R> s;
-  sincos_t(thB, &s.sth, &s.cth);
+  s.sth = sth;
+  s.cth = cth;
   s.te = te;
   s.ite = R(1) / te;
-  s.inu_c = R(1) / (R(NU_CRIT) * B * s.sth * te * te);
+  s.inu_c = fastm::div(R(1), R(NU_CRIT) * B * s.sth * te * te);
   s.jpre = R(JNU) * ne * s.ite * s.ite;
   if (s.ite < R(1.0 / 5.0)) {
     // Theta_e > 5: K_nu(x) -> 2^(nu-1) (nu-1)! x^-nu (nu > 0), K_0 -> -ln(x/2) - gamma_E
@@ -141,35 +143,39 @@ PHX_HD Coeffs<R> synchro_coeffs(const SynchroSample<R>& s, R nu, R jscale) {
   Coeffs<R> c;
   // emissivity fits in x = nu / nu_c
   const R x = nu * s.inu_c;
-  const R cx = cbrt_t(x), icx = R(1) / cx;
-  const R ex = exp_t(R(-1.8899) * cx);
+  // cbrt stays accurate: exp(-1.8899 cbrt(x)) multiplies its relative error by 1.89 cbrt(x) ~ 10..100
+  const R cx = cbrt_t(x), icx = fastm::div(R(1), cx);
+  const R ex = fastm::exp(R(-1.8899) * cx);
   const R pref = s.jpre * nu;
   const R II = R(2.5651) * (R(1) + R(1.92) * icx + R(0.9977) * icx * icx) * ex;
   const R IQ = R(2.5651) * (R(1) + R(0.93193) * icx + R(0.499873) * icx * icx) * ex;
-  const R IV = (R(1.81348) * icx * icx * icx + R(3.42319) * icx * icx + R(0.0292545) / sqrt_t(x) + R(2.03773) * icx) * ex;
+  const R IV = (R(1.81348) * icx * icx * icx + R(3.42319) * icx * icx + fastm::div(R(0.0292545), sqrt_t(x)) +
+                R(2.03773) * icx) * ex;
   R jI = pref * II;
   R jQ = pref * IQ;
-  R jV = R(4.0 / 3.0) * pref * s.ite * (s.cth / s.sth) * IV;
+  R jV = R(4.0 / 3.0) * pref * s.ite * fastm::div(s.cth, s.sth) * IV;
   // Kirchhoff: alpha = j / B_nu(Theta_e)
   const R pre = R(2.0 * cgs::h_planck) * nu * nu * nu / R(cgs::c_light * cgs::c_light);
   const R xx = R(H_OVER_MEC2) * nu * s.ite;
-  const R iB = (sizeof(R) == 4 ? expm1_t(xx) : (exp_t(xx) - R(1))) / pre;
+  const R iB = fastm::div(sizeof(R) == 4 ? expm1_t(xx) : (exp_t(xx) - R(1)), pre);
   R aI = jI * iB, aQ = jQ * iB, aV = jV * iB;
   // Faraday rotation / conversion
-  const R iw = R(1) / (R(kTwoPi) * nu);
-  const R Xe = s.te * sqrt_t(R(1.4142135623730951) * s.sth * (R(1e3 / kTwoPi) * s.omega0 / nu));
-  const R lx = log_t(Xe);
-  const R exm = exp_t(-Xe / R(47.2));
-  const R fm = R(2.011) * exp_t(-exp_t(R(1.035) * lx) / R(4.7)) - cos_t(Xe * R(0.5)) * exp_t(-exp_t(R(1.2) * lx) / R(2.73)) -
-               R(0.011) * exm +
-               (R(0.011) * exm - R(C0) * exp_t(R(-8.0 / 3.0) * lx)) * R(0.5) * (R(1) + tanh_t(R(10) * (lx - R(LOG120))));
+  const R iw = fastm::div(R(1), R(kTwoPi) * nu);
+  const R Xe = s.te * sqrt_t(R(1.4142135623730951) * s.sth * fastm::div(R(1e3 / kTwoPi) * s.omega0, nu));
+  const R lx = fastm::log(Xe);
+  const R exm = fastm::exp(-Xe * R(1.0 / 47.2));
+  const R fm = R(2.011) * fastm::exp(-fastm::exp(R(1.035) * lx) * R(1.0 / 4.7)) -
+               fastm::cos(Xe * R(0.5)) * fastm::exp(-fastm::exp(R(1.2) * lx) * R(1.0 / 2.73)) - R(0.011) * exm +
+               (R(0.011) * exm - R(C0) * fastm::exp(R(-8.0 / 3.0) * lx)) * R(0.5) *
+                   (R(1) + fastm::tanh(R(10) * (lx - R(LOG120))));
   const R q = s.omega0 * iw;
   const R wpw = s.wp2 * iw;
   R rQ = R(0.5 / cgs::c_light) * wpw * q * q * fm * (s.kr1 + R(6) * s.te) * s.sth * s.sth;
-  const R shgm = R(1) - R(0.11) * log_t(R(1) + R(0.035) * Xe);
+  const R shgm = R(1) - R(0.11) * fastm::log(R(1) + R(0.035) * Xe);
   R rV = R(1.0 / cgs::c_light) * wpw * q * (s.kr0 * shgm) * s.cth;
   // invariant form (nu is the plasma-frame frequency here)
-  const R js = jscale / nu / nu;
+  const R inu = fastm::div(R(1), nu);
+  const R js = jscale * inu * inu;
   jI *= js;
   jQ *= js;
   jV *= js;
@@ -178,10 +184,11 @@ PHX_HD Coeffs<R> synchro_coeffs(const SynchroSample<R>& s, R nu, R jscale) {
   aV *= nu;
   rQ *= nu;
   rV *= nu;
-  const R pf = sqrt_t(jQ * jQ + jV * jV) / jI;
+  const R pf = fastm::div(sqrt_t(jQ * jQ + jV * jV), jI);
   if (pf > R(1)) {
-    jQ /= (pf + R(0.005));
-    jV /= (pf + R(0.005));
+    const R ipf = fastm::div(R(1), pf + R(0.005));
+    jQ *= ipf;
+    jV *= ipf;
   }
   c.jI = jI; c.jQ = jQ; c.jV = jV;
   c.aI = aI; c.aQ = aQ; c.aV = aV;

@@ -113,6 +113,14 @@ phx::SnapView<R, PT> snap_view(const PhxSnapshot* s, const R* lb, const R* dxc, 
   v.a = R(s->a);
   v.hs = R(s->hslope);
   v.gam = R(s->gam);
+  v.lbd = s->lb_d;
+  v.dxcd = s->dxc_d;
+  for (int d = 0; d < 3; d++) {
+    v.xlo_d[1 + d] = s->x_lo[d];
+    v.xhi_d[1 + d] = s->x_hi[d];
+    v.w0_d[d] = (s->x_hi[d] - s->x_lo[d]) / s->ng[d];
+  }
+  v.xlo_d[0] = v.xhi_d[0] = 0.0;
   return v;
 }
 
