@@ -32,9 +32,29 @@ REF_CPU = os.path.join(ROOT, "oracle", "_ref", "ref_render_fp32")
 
 WORKLOAD = dict(base=(192, 96, 96), nlevels=3, refine=(3.5, 25.0, 0.55), seed=0, img=512,
                 inclinations=(10.0, 60.0, 163.0), frequency=230e9, m_unit=1.2e18)
-# Algorithmic FP32 flops per unit of work ("Roofline"): per ray-step, per plasma sample, per
-# (sample, frequency).
+# Algorithmic FP32 flops per unit of work: per ray-step (RK4 with four metric/Christoffel evaluations, step size),
+# per emitting sample (metric, fluid, tetrad, pitch angle), per (sample, frequency) (coefficients, segment operator,
+# accumulation).  Op-count estimates of the reference path, frozen here so that every run uses the same figures.
 FLOPS = dict(step=1800.0, sample=900.0, freq=850.0)
+# Algorithmic bytes the march requests from the memory system: per emitting sample the 8 corners x 8 FP32 primitives
+# of the trilinear gather (256 B); per step the flattened leaf-map entry (4 B) and the leaf's lb/dxc (24 B); per ray
+# its job index (4 B) and one 48 B FreqOut record per frequency.
+BYTES = dict(sample=256.0, step=28.0, ray=4.0, ray_freq=48.0)
+# DRAM bytes (read + write) per ray-step of k_march, from the ncu capture of the same snapshot at 256^2 pixels
+# (profiles/k_march_plain_gpu_256.md): dram__bytes_read.sum + dram__bytes_write.sum = 572.5 MB over the launch's
+# ~197M ray-steps.  Scaled to a full launch by its ray-steps.
+DRAM_BYTES_PER_STEP = 2.90
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+
+def measured_peaks():
+    """HBM copy bandwidth measured on this pool's B200s, else the earlier measurement (6.65 TB/s)."""
+    try:
+        with open(PEAKS_FILE) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
 
 
 def log(*a):
@@ -272,6 +292,7 @@ def main():
                 ev[s][1].record(stream)
             stream.synchronize()
             c = ctr.cpu().numpy()
+            steps_per_launch = [int(v) for v in c[:, P.CTR["steps"]]]
             steps_total += int(c[:, P.CTR["steps"]].sum())
             nplasma_total += int(c[:, P.CTR["nplasma"]].sum())
         torch.cuda.synchronize()
@@ -315,11 +336,18 @@ def main():
     if rank == 0:
         nimg = len(params) * args.steps
         nfreq = 1
+        nlaunch = len(kms)
+        kavg_s = sum(kms) / nlaunch * 1e-3
         flops = FLOPS["step"] * steps_total + (FLOPS["sample"] + nfreq * FLOPS["freq"]) * nplasma_total
-        kavg = sum(kms) / len(kms)
-        achieved = flops / len(kms) / (kavg * 1e-3) / 1e12
+        fp32_achieved = flops / nlaunch / kavg_s / 1e12
         props = torch.cuda.get_device_properties(dev)
-        peak = props.multi_processor_count * 128 * 2 * 1.965e9 / 1e12
+        fp32_peak = props.multi_processor_count * 128 * 2 * 1.965e9 / 1e12
+        rays = nimg * npix
+        nbytes = (BYTES["sample"] * nplasma_total + BYTES["step"] * steps_total +
+                  (BYTES["ray"] + nfreq * BYTES["ray_freq"]) * rays)
+        hbm_achieved = nbytes / nlaunch / kavg_s / 1e9
+        hbm_peak, peak_kind = measured_peaks()
+        traffic = None if DRAM_BYTES_PER_STEP is None else DRAM_BYTES_PER_STEP * steps_total / nlaunch
         line = {
             "metric": "ray-steps/s", "value": value, "unit": "ray-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -333,12 +361,20 @@ def main():
             "images_per_s": nimg / (ms_max * 1e-3) * world,
             "rays_per_s": nimg * npix / (ms_max * 1e-3) * world,
             "ray_steps_per_step": steps_total / args.steps,
-            "gpu_launches": len(kms),
-            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": None,
-                         "note": "FP32-issue roofline: algorithmic flops per launch (per-step/sample/frequency "
-                                 "constants) over the average launch time; peak = SMs x 128 lanes x 2 x 1965 MHz "
-                                 "(nominal; no measured FP32 peak exists for this pool)"},
+            "ray_steps_per_launch": steps_per_launch,
+            "gpu_launches": nlaunch,
+            "roofline": {"bound": "hbm", "achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": hbm_achieved / hbm_peak, "traffic": traffic,
+                         "kernel": "k_march", "launch_ms": kavg_s * 1e3, "algorithmic_bytes_per_launch": nbytes / nlaunch,
+                         "note": f"secondary roofline ({peak_kind} HBM copy peak): the bytes the march requests "
+                                 "(256 B gather per emitting sample, 28 B leaf lookup per step, 52 B per ray) per "
+                                 "launch over the CUDA-event launch time; most hit L1/L2, traffic is the DRAM share. "
+                                 "The kernel is FP32-issue bound: see roofline_fp32"},
+            "roofline_fp32": {"bound": "fp32", "achieved": fp32_achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                              "frac": fp32_achieved / fp32_peak,
+                              "note": "algorithmic flops per launch (1800 per step, 900 per emitting sample, 850 per "
+                                      "sample-frequency) over the launch time; peak = SMs x 128 FP32 lanes x 2 x "
+                                      "1965 MHz (nominal, no measured FP32 peak for this pool)"},
             "clocks": clocks,
             "e2e": e2e,
         }

@@ -96,9 +96,9 @@ typedef struct {
   double r_fp64;       /* mixed: FP64 RK4 inside r < r_fp64 * r_horizon (<= 0: default 1.5) */
   double tau_fp64;     /* mixed: FP64 segment operator where h max|K| exceeds this (<= 0: default 0.1) */
   int32_t block;       /* threads per block, 0 = default */
-  int32_t period;      /* march passes between lane refills, 0 = default (16) */
+  int32_t period;      /* march passes between lane refills, 0 = default (32) */
   int32_t blocks_per_sm; /* register-cap variant: resident 128-thread blocks per SM the kernel is compiled for
-                            (1: up to 255 registers, 3: 168, 4: 128); 0 = default (4 for one frequency, else 3) */
+                            (1: up to 255 registers, 3: 168, 4: 128); 0 = default (3) */
 } PhxRenderParams;
 
 /* What a render reports (a superset of the reference's device::Info, src/device/kernel.cuh:23-30). */

@@ -129,7 +129,7 @@ def test_frequencies_are_independent(gpu_snapshots):
         assert np.abs(multi[:, :, f] - single[:, :, 0]).max() <= 1e-12 * scale
 
 
-@pytest.mark.parametrize("bps", [0, 1, 3])
+@pytest.mark.parametrize("bps", [0, 1, 4])
 def test_results_independent_of_scheduling(gpu_snapshots, bps):
     """A ray's arithmetic does not depend on which lane, warp or refill round runs it: for one compiled variant the
     image is bit-identical whatever the refill period.  Variants compiled for other register caps round differently
