@@ -61,19 +61,23 @@ def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
-def snapshot_files(w=WORKLOAD, root=None):
-    """Generate (once per machine) the workload's snapshot; returns (dump, grid)."""
-    key = hashlib.sha1(json.dumps([w["base"], w["nlevels"], w["refine"], w["seed"]]).encode()).hexdigest()[:12]
+def generated_snapshot(gen_args, root=None):
+    """Generate (once per machine) a synthetic BHAC snapshot with phx_gen_snapshot; returns (dump, grid)."""
+    key = hashlib.sha1(json.dumps(list(gen_args)).encode()).hexdigest()[:12]
     d = os.path.join(root or tempfile.gettempdir(), "phx_bench_" + key)
     dump, grid = os.path.join(d, "dump.dat"), os.path.join(d, "grid.in")
     done = os.path.join(d, "done")
     if not os.path.exists(done):
         os.makedirs(d, exist_ok=True)
-        args = [GEN, "--out", d, "--seed", str(w["seed"]), "--base", *map(str, w["base"]), "--nlevels",
-                str(w["nlevels"]), "--nws", "0", "--refine", *map(str, w["refine"])]
-        subprocess.check_call(args, stdout=subprocess.DEVNULL)
+        subprocess.check_call([GEN, "--out", d] + list(gen_args), stdout=subprocess.DEVNULL)
         open(done, "w").close()
     return dump, grid
+
+
+def snapshot_files(w=WORKLOAD, root=None):
+    """The plain-path workload's snapshot; returns (dump, grid)."""
+    return generated_snapshot(["--seed", str(w["seed"]), "--base", *map(str, w["base"]), "--nlevels",
+                               str(w["nlevels"]), "--nws", "0", "--refine", *map(str, w["refine"])], root)
 
 
 def render_kwargs(w=WORKLOAD):
@@ -212,6 +216,111 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# Batching workload: 128 images over the 64x32x32-base snapshot (3 levels, seed 0), drawn from seed 7.
+BATCH = dict(gen=["--seed", "0", "--base", "64", "32", "32", "--nlevels", "3"], nlevels=3, nimages=128, seed=7,
+             resolutions=(64, 128, 256, 512), incl=(5.0, 175.0), freq=(86e9, 690e9), m_unit=(1e17, 1e19))
+
+
+def batch_images(b=BATCH):
+    """The seeded image list: resolution uniform over the set, inclination uniform, frequency and m_unit
+    log-uniform."""
+    rng = np.random.default_rng(b["seed"])
+    n = b["nimages"]
+    res = rng.choice(b["resolutions"], n)
+    inc = rng.uniform(*b["incl"], n)
+    fr = np.exp(rng.uniform(np.log(b["freq"][0]), np.log(b["freq"][1]), n))
+    mu = np.exp(rng.uniform(np.log(b["m_unit"][0]), np.log(b["m_unit"][1]), n))
+    return [dict(img=int(res[k]), inclination=float(inc[k]), frequencies=[float(fr[k])], m_unit=float(mu[k]))
+            for k in range(n)]
+
+
+def run_batch(args):
+    """Config 4: the 128-image sweep rendered one by one with the plain single-image path (FP32) and as one batch
+    (FP32, mixed and FP64; autotuned launch shape).  Device-resident inputs, CUDA-event timing, L2 flushed between
+    timed repetitions.  Prints one JSON line."""
+    import torch
+
+    import phoenix_b200 as P
+    dev = torch.device("cuda", 0)
+    dump, grid = generated_snapshot(BATCH["gen"])
+    snap = P.Snapshot.load(dump, grid, nlevels=BATCH["nlevels"], f64_prims=True)
+    imgs = batch_images()
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    K, W = max(1, args.steps), max(1, args.warmup)
+
+    def timed(fn):
+        ts = []
+        for r in range(W + K):
+            with torch.cuda.stream(stream):
+                flush.fill_(r & 0xFF)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+            stream.synchronize()
+            if r >= W:
+                ts.append(e0.elapsed_time(e1))
+        return ts
+
+    # plain path, one launch per image
+    params = [P.make_params(precision="fp32", **im) for im in imgs]
+    jobs = {r: torch.from_numpy(P.schedule_morton(r, r)).to(dev) for r in BATCH["resolutions"]}
+    outs = [torch.zeros((p.img_width * p.img_height, 1, 6), dtype=torch.float64, device=dev) for p in params]
+    ctr = torch.zeros((len(params), P.NUM_COUNTERS), dtype=torch.int64, device=dev)
+
+    def plain():
+        ctr.zero_()
+        for k, p in enumerate(params):
+            j = jobs[p.img_width]
+            snap.render_async(p, j.data_ptr(), j.numel(), outs[k].data_ptr(), ctr[k].data_ptr(), 0, stream.cuda_stream)
+
+    t_plain = timed(plain)
+    steps = int(ctr[:, P.CTR["steps"]].sum())
+    rays = sum(p.img_width * p.img_height for p in params)
+    line = {"workload": "batch", "metric": "ray-steps/s", "unit": "ray-steps/s", "n_gpus": 1, "steps": K,
+            "warmup": W, "data": "synthetic",
+            "config": {"snapshot": "64x32x32 base grid, 8^3 blocks, 3 AMR levels, seed 0", "images": len(imgs),
+                       "image_seed": BATCH["seed"], "resolutions": list(BATCH["resolutions"]), "rays": rays,
+                       "l2": "flushed (256 MB write) before every timed repetition"},
+            "ray_steps": steps}
+    ms = min(t_plain)
+    line["plain_fp32"] = {"ms": ms, "ray_steps_per_s": steps / (ms * 1e-3), "images_per_s": len(imgs) / (ms * 1e-3),
+                          "launches": len(imgs)}
+    fluxes = {}
+    for prec in ("fp32", "mixed", "fp64"):
+        items = [(snap, P.make_params(precision=prec, **im)) for im in imgs]
+        t0 = time.time()
+        b = P.Batch(items, autotune=not args.no_autotune)
+        create_s = time.time() - t0
+        ts = timed(lambda: b.launch(stream.cuda_stream))
+        tune = b.tuning()
+        ms = min(ts)
+        bsteps = 0
+        fl = []
+        for k in range(len(items)):
+            res, info = b.result(k)
+            bsteps += info["steps"]
+            fl.append(P.flux(res, items[k][1])[0])
+        fluxes[prec] = np.array(fl)
+        line["batch_" + prec] = {"ms": ms, "ray_steps_per_s": bsteps / (ms * 1e-3),
+                                 "images_per_s": len(imgs) / (ms * 1e-3), "launches": 2,
+                                 "create_s": create_s, "tuning": {k: tune[k] for k in
+                                                                  ("blocks_per_sm", "period", "tile_rays", "grid",
+                                                                   "regs", "ntiles", "device_bytes")},
+                                 "candidates": tune["candidates"], "ray_steps": bsteps}
+        b.close()
+    ref = fluxes["fp64"]
+    for prec in ("fp32", "mixed"):
+        err = np.abs(fluxes[prec] - ref) / np.abs(ref[:, :1])
+        line["batch_" + prec]["flux_err_vs_fp64"] = {"I_max": float(err[:, 0].max()),
+                                                     "QUV_max": float(err[:, 1:].max())}
+    pl = line["plain_fp32"]["ray_steps_per_s"]
+    line["speedup_vs_plain_fp32"] = {p: line["batch_" + p]["ray_steps_per_s"] / pl for p in ("fp32", "mixed", "fp64")}
+    snap.close()
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -223,9 +332,14 @@ def main():
     ap.add_argument("--period", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="plain", choices=["plain", "batch"],
+                    help="plain: the headline single-image path (default); batch: the 128-image sweep")
+    ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batch":
+        return run_batch(args)
 
     import torch
     import torch.distributed as dist

@@ -170,6 +170,66 @@ int phx_render_async(PhxSnapshot* s, const PhxRenderParams* p, const int32_t* d_
 int phx_render_noalloc(PhxSnapshot* s, const PhxRenderParams* p, const int32_t* jobs, int64_t njobs,
                        PhxFreqOut* d_res, void* stream);
 
+/* ---- Batches: many images in one persistent, graph-captured launch ----
+ * No single reference counterpart: the reference renders one image per device::render call
+ * (src/device/kernel.cu:284-360, called once from src/main.cpp:186-187); a batch renders many such calls' images --
+ * any mix of snapshots, resolutions, inclinations, frequencies and plasma parameters -- in one launch of a queue-fed
+ * kernel whose lanes take rays from a device work queue of ray tiles, so that short images do not leave the GPU idle
+ * while long rays finish.  Every item's result equals what phx_render returns for the same parameters, to the
+ * rounding of the separately compiled kernel (and bit for bit across batches, whatever the mix). */
+typedef struct PhxBatch PhxBatch;
+
+typedef struct {
+  PhxSnapshot* snapshot;   /* resident snapshot (all items on one device) */
+  PhxRenderParams params;  /* one image; `precision` must agree across the batch; at most 4 frequencies unless FP32 */
+  const int32_t* jobs;     /* host job list (copied at creation), or NULL: every pixel in Morton order */
+  int64_t njobs;
+} PhxBatchItem;
+
+typedef struct {
+  int32_t tile_rays;       /* rays per queue tile, 0 = 32 */
+  int32_t blocks_per_sm;   /* register-cap variant (FP32: 1, 3, 4), 0 = default 3 or autotuned */
+  int32_t period;          /* march passes between lane refills, 0 = default 32 or autotuned */
+  int32_t autotune;        /* nonzero: time every (blocks_per_sm, period) candidate on a sample of the batch's tiles
+                              at creation and keep the fastest */
+  int32_t sample_stride;   /* autotune sample: every n-th tile, 0 = 16 */
+  int32_t keep_order;      /* nonzero: tiles in item order; 0: the largest images' tiles first */
+} PhxBatchOptions;
+
+#define PHX_TUNE_MAX_CANDIDATES 16
+typedef struct {
+  int32_t blocks_per_sm, period, tile_rays;
+  int32_t grid, block, regs, local_bytes;
+  int32_t ncand;  /* candidates timed by the autotuner (0 if it did not run) */
+  int32_t cand_blocks_per_sm[PHX_TUNE_MAX_CANDIDATES], cand_period[PHX_TUNE_MAX_CANDIDATES];
+  double cand_ms[PHX_TUNE_MAX_CANDIDATES];
+  int64_t nitems, ntiles, nrays;
+  int64_t device_bytes;  /* device memory the batch holds (tables, job lists, results) */
+} PhxBatchTuning;
+
+void phx_default_batch_options(PhxBatchOptions* o);
+
+/* Uploads the items' constants and job lists, allocates their device results, optionally autotunes, and captures the
+ * launch (queue reset + kernel) in a CUDA graph. */
+int phx_batch_create(const PhxBatchItem* items, int32_t nitems, const PhxBatchOptions* opt, PhxBatch** out);
+
+/* Replays the captured launch on `stream` (cudaStream_t as void*, NULL = default stream).  Asynchronous. */
+int phx_batch_launch(PhxBatch* b, void* stream);
+
+/* Launch on the batch's own stream, wait, and record the kernel time (reported by phx_batch_result). */
+int phx_batch_run(PhxBatch* b);
+
+/* After a launch has completed: item `item`'s records into host memory res (img_width * img_height * nfreqs
+ * records; pixels outside its job list are zero) and its counters into info (NULL allowed). */
+int phx_batch_result(PhxBatch* b, int32_t item, PhxFreqOut* res, PhxRenderInfo* info);
+
+/* Device address of item `item`'s records (valid until phx_batch_destroy). */
+int phx_batch_device_result(PhxBatch* b, int32_t item, PhxFreqOut** d_res);
+
+int phx_batch_tuning(const PhxBatch* b, PhxBatchTuning* t);
+
+void phx_batch_destroy(PhxBatch* b);
+
 /* Writes a render's outputs the way PHOENIX's write_output does (src/main.cpp:52-86, src/host/io/output.hpp):
  * `image` = "hdf5" -> outdir/img_data.h5 (RAPTOR block layout, block_size pixels per side; if it cannot be written the
  * text image is written instead), "text" -> outdir/image.dat (image_<f>.dat per frequency when nfreqs > 1),

@@ -16,7 +16,7 @@ from . import native
 from .native import (CTR, NUM_COUNTERS, PREC_FP32, PREC_FP64, PREC_MIXED, PhxError, PhxRenderInfo, make_params,
                      schedule_morton, write_output)
 
-__all__ = ["Snapshot", "make_params", "schedule_morton", "write_output", "flux", "pixel_solid_angle", "PhxError", "PREC_FP32",
+__all__ = ["Snapshot", "Batch", "make_params", "schedule_morton", "write_output", "flux", "pixel_solid_angle", "PhxError", "PREC_FP32",
            "PREC_FP64", "PREC_MIXED", "CTR", "NUM_COUNTERS"]
 
 G_GRAV, M_SUN, C_LIGHT, KPC, JANSKY = 6.674e-8, 1.989e33, 2.99792458e10, 3.086e21, 1e23
@@ -97,6 +97,77 @@ class Snapshot:
     def close(self):
         if self._h and self._h.value:
             native.lib().phx_snapshot_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many images (any mix of snapshots, resolutions, cameras, frequencies and plasma parameters, one precision)
+    rendered by one persistent, graph-captured launch of the queue kernel.  items: (snapshot, params) or
+    (snapshot, params, jobs) tuples."""
+
+    def __init__(self, items, tile_rays=32, blocks_per_sm=0, period=0, autotune=False, sample_stride=16,
+                 keep_order=False):
+        L = native.lib()
+        n = len(items)
+        arr = (native.PhxBatchItem * n)()
+        self._keep = []
+        self.params = []
+        for k, it in enumerate(items):
+            snap, p = it[0], it[1]
+            jobs = it[2] if len(it) > 2 else None
+            arr[k].snapshot = snap.handle.value
+            arr[k].params = p
+            if jobs is not None:
+                j = np.ascontiguousarray(jobs, dtype=np.int32)
+                self._keep.append(j)
+                arr[k].jobs, arr[k].njobs = j.ctypes.data, j.size
+            self.params.append(p)
+        o = native.PhxBatchOptions(tile_rays, blocks_per_sm, period, 1 if autotune else 0, sample_stride,
+                                   1 if keep_order else 0)
+        h = C.c_void_p()
+        native.check(L.phx_batch_create(arr, n, C.byref(o), C.byref(h)))
+        self._h = h
+
+    def launch(self, stream: int = 0):
+        """Replay the captured launch on a CUDA stream (asynchronous)."""
+        native.check(native.lib().phx_batch_launch(self._h, stream or None))
+
+    def run(self):
+        """Launch on the batch's own stream and wait."""
+        native.check(native.lib().phx_batch_run(self._h))
+
+    def result(self, item: int):
+        p = self.params[item]
+        res = np.zeros((p.img_width, p.img_height, p.nfreqs, 6), dtype=np.float64)
+        info = PhxRenderInfo()
+        native.check(native.lib().phx_batch_result(self._h, item, res.ctypes.data, C.byref(info)))
+        return res, info.as_dict()
+
+    def device_result(self, item: int) -> int:
+        ptr = C.c_void_p()
+        native.check(native.lib().phx_batch_device_result(self._h, item, C.byref(ptr)))
+        return ptr.value
+
+    def tuning(self) -> dict:
+        t = native.PhxBatchTuning()
+        native.check(native.lib().phx_batch_tuning(self._h, C.byref(t)))
+        return t.as_dict()
+
+    def close(self):
+        if self._h and self._h.value:
+            native.lib().phx_batch_destroy(self._h)
             self._h = C.c_void_p()
 
     def __enter__(self):

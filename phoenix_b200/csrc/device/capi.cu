@@ -17,112 +17,12 @@
 #include "../host/output.hpp"
 #include "../host/render_setup.hpp"
 #include "../host/snapshot.hpp"
+#include "internal.hpp"
 #include "march.cuh"
 
-namespace {
-
-thread_local std::string g_err;
-
-int fail(int code, const std::string& msg) {
-  g_err = msg;
-  return code;
-}
-
-struct CudaError : std::runtime_error {
-  explicit CudaError(const std::string& m) : std::runtime_error(m) {}
-};
-
-void ck(cudaError_t e, const char* what) {
-  if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
-}
-
-template <class T>
-T* dev_upload(const T* host, size_t n, std::vector<void*>& owned) {
-  T* d = nullptr;
-  ck(cudaMalloc((void**)&d, std::max<size_t>(n, 1) * sizeof(T)), "cudaMalloc");
-  owned.push_back(d);
-  if (n) ck(cudaMemcpy(d, host, n * sizeof(T), cudaMemcpyHostToDevice), "cudaMemcpy H2D");
-  return d;
-}
-
-// Device workspace of the synchronous render entry (grown on demand, reused across calls).
-struct Workspace {
-  int32_t* jobs = nullptr;
-  size_t jobs_cap = 0;
-  PhxFreqOut* res = nullptr;
-  size_t res_cap = 0;
-  unsigned long long* counters = nullptr;
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  ~Workspace() {
-    cudaFree(jobs);
-    cudaFree(res);
-    cudaFree(counters);
-    if (e0) cudaEventDestroy(e0);
-    if (e1) cudaEventDestroy(e1);
-  }
-};
-
-}  // namespace
-
-struct PhxHostSnapshot {
-  phx::HostSnapshot h;
-  std::vector<const int32_t*> maps;
-};
-
-struct PhxSnapshot {
-  int device = 0;
-  int sms = 0;
-  char device_name[256] = {0};
-  int32_t nleafs = 0, nlevels = 0, cells = 0;
-  int32_t nx[3] = {0, 0, 0}, ng[3] = {0, 0, 0}, fd[3] = {0, 0, 0};
-  double a = 0, hslope = 0, gam = 0;
-  double x_lo[3] = {0, 0, 0}, x_hi[3] = {0, 0, 0};
-  float *lb_f = nullptr, *dxc_f = nullptr, *prim_f = nullptr;
-  double *lb_d = nullptr, *dxc_d = nullptr, *prim_d = nullptr;
-  int32_t* fmap = nullptr;
-  int64_t bytes = 0;
-  std::vector<void*> owned;
-  Workspace ws;
-  cudaStream_t stream = nullptr;
-  ~PhxSnapshot() {
-    if (stream) cudaStreamDestroy(stream);
-    for (void* p : owned) cudaFree(p);
-  }
-};
+using namespace phx_capi;
 
 namespace {
-
-template <class R, class PT>
-phx::SnapView<R, PT> snap_view(const PhxSnapshot* s, const R* lb, const R* dxc, const PT* prim) {
-  phx::SnapView<R, PT> v;
-  v.lb = lb;
-  v.dxc = dxc;
-  v.prim = prim;
-  v.fmap = s->fmap;
-  for (int d = 0; d < 3; d++) {
-    v.fd[d] = s->fd[d];
-    v.nx[d] = s->nx[d];
-    v.x_lo[1 + d] = R(s->x_lo[d]);
-    v.x_hi[1 + d] = R(s->x_hi[d]);
-    v.w0[d] = R((s->x_hi[d] - s->x_lo[d]) / s->ng[d]);
-  }
-  v.x_lo[0] = v.x_hi[0] = R(0);
-  v.nleafs = s->nleafs;
-  v.nlevels = s->nlevels;
-  v.cells = s->cells;
-  v.a = R(s->a);
-  v.hs = R(s->hslope);
-  v.gam = R(s->gam);
-  v.lbd = s->lb_d;
-  v.dxcd = s->dxc_d;
-  for (int d = 0; d < 3; d++) {
-    v.xlo_d[1 + d] = s->x_lo[d];
-    v.xhi_d[1 + d] = s->x_hi[d];
-    v.w0_d[d] = (s->x_hi[d] - s->x_lo[d]) / s->ng[d];
-  }
-  v.xlo_d[0] = v.xhi_d[0] = 0.0;
-  return v;
-}
 
 template <phx::Mode M, class PT>
 cudaError_t launch_mode(PhxSnapshot* s, const PhxRenderParams& p, const typename phx::Policy<M>::R* lb,
@@ -230,21 +130,6 @@ PhxSnapshot* create_snapshot(const PhxSnapshotDesc* d, int32_t flags) {
                        (s->prim_d ? nprim * sizeof(double) : 0) + flat.size() * sizeof(int32_t));
   ck(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
   return s.release();
-}
-
-template <class F>
-int guarded(F&& f) {
-  try {
-    return f();
-  } catch (const CudaError& e) {
-    return fail(PHX_E_CUDA, e.what());
-  } catch (const std::invalid_argument& e) {
-    return fail(PHX_E_INVALID, e.what());
-  } catch (const std::bad_alloc&) {
-    return fail(PHX_E_INVALID, "host allocation failed");
-  } catch (const std::exception& e) {
-    return fail(PHX_E_IO, e.what());
-  }
 }
 
 }  // namespace
@@ -390,7 +275,7 @@ int phx_render(PhxSnapshot* s, const PhxRenderParams* p, const int32_t* jobs, in
     std::vector<int32_t> all;
     if (!jobs) {
       all.resize(npix);
-      if (phx_schedule_morton(p->img_width, p->img_height, all.data()) != PHX_OK) throw std::runtime_error(g_err);
+      if (phx_schedule_morton(p->img_width, p->img_height, all.data()) != PHX_OK) throw std::runtime_error(last_error());
       jobs = all.data();
       njobs = npix;
     }
@@ -479,7 +364,7 @@ int phx_write_output(const PhxRenderParams* p, const PhxFreqOut* res, const char
   });
 }
 
-const char* phx_last_error(void) { return g_err.c_str(); }
+const char* phx_last_error(void) { return last_error().c_str(); }
 
 const char* phx_version(void) { return "phoenix-b200 0.1 (sm_100a)"; }
 

@@ -26,7 +26,9 @@ CTR = dict(queue=0, steps=1, nplasma=2, bad=3, scans=4, fp64_steps=5, fp64_ops=6
 # Every symbol include/phoenix_b200.h declares.
 EXPORTS = ["phx_default_params", "phx_snapshot_create", "phx_snapshot_load", "phx_snapshot_destroy",
            "phx_bhac_read", "phx_bhac_describe", "phx_bhac_free", "phx_snapshot_bytes", "phx_schedule_morton", "phx_render", "phx_render_async", "phx_render_noalloc", "phx_write_output", "phx_last_error",
-           "phx_version"]
+           "phx_version", "phx_default_batch_options", "phx_batch_create", "phx_batch_launch", "phx_batch_run",
+           "phx_batch_result", "phx_batch_device_result", "phx_batch_tuning", "phx_batch_destroy"]
+TUNE_MAX_CANDIDATES = 16
 
 
 class PhxFreqOut(C.Structure):
@@ -76,6 +78,32 @@ class PhxRenderInfo(C.Structure):
         return d
 
 
+class PhxBatchItem(C.Structure):
+    _fields_ = [("snapshot", C.c_void_p), ("params", PhxRenderParams), ("jobs", C.c_void_p), ("njobs", C.c_int64)]
+
+
+class PhxBatchOptions(C.Structure):
+    _fields_ = [("tile_rays", C.c_int32), ("blocks_per_sm", C.c_int32), ("period", C.c_int32),
+                ("autotune", C.c_int32), ("sample_stride", C.c_int32), ("keep_order", C.c_int32)]
+
+
+class PhxBatchTuning(C.Structure):
+    _fields_ = [
+        ("blocks_per_sm", C.c_int32), ("period", C.c_int32), ("tile_rays", C.c_int32),
+        ("grid", C.c_int32), ("block", C.c_int32), ("regs", C.c_int32), ("local_bytes", C.c_int32),
+        ("ncand", C.c_int32), ("cand_blocks_per_sm", C.c_int32 * TUNE_MAX_CANDIDATES),
+        ("cand_period", C.c_int32 * TUNE_MAX_CANDIDATES), ("cand_ms", C.c_double * TUNE_MAX_CANDIDATES),
+        ("nitems", C.c_int64), ("ntiles", C.c_int64), ("nrays", C.c_int64), ("device_bytes", C.c_int64),
+    ]
+
+    def as_dict(self):
+        n = self.ncand
+        d = {name: getattr(self, name) for name, _ in self._fields_ if not name.startswith("cand_")}
+        d["candidates"] = [dict(blocks_per_sm=self.cand_blocks_per_sm[i], period=self.cand_period[i],
+                                ms=self.cand_ms[i]) for i in range(n)]
+        return d
+
+
 class PhxError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"phoenix_b200 error {code}: {msg}")
@@ -115,8 +143,19 @@ def lib():
     L.phx_write_output.restype = C.c_int
     L.phx_last_error.restype = C.c_char_p
     L.phx_version.restype = C.c_char_p
+    L.phx_default_batch_options.argtypes = [P(PhxBatchOptions)]
+    L.phx_default_batch_options.restype = None
+    L.phx_batch_create.argtypes = [P(PhxBatchItem), C.c_int32, P(PhxBatchOptions), P(C.c_void_p)]
+    L.phx_batch_launch.argtypes = [C.c_void_p, C.c_void_p]
+    L.phx_batch_run.argtypes = [C.c_void_p]
+    L.phx_batch_result.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, P(PhxRenderInfo)]
+    L.phx_batch_device_result.argtypes = [C.c_void_p, C.c_int32, P(C.c_void_p)]
+    L.phx_batch_tuning.argtypes = [C.c_void_p, P(PhxBatchTuning)]
+    L.phx_batch_destroy.argtypes = [C.c_void_p]
+    L.phx_batch_destroy.restype = None
     for name in ("phx_snapshot_create", "phx_snapshot_load", "phx_bhac_read", "phx_bhac_describe", "phx_schedule_morton",
-                 "phx_render", "phx_render_async", "phx_render_noalloc"):
+                 "phx_render", "phx_render_async", "phx_render_noalloc", "phx_batch_create", "phx_batch_launch",
+                 "phx_batch_run", "phx_batch_result", "phx_batch_device_result", "phx_batch_tuning"):
         getattr(L, name).restype = C.c_int
     _lib = L
     return L

@@ -81,3 +81,15 @@ def oracle_results(snapshots):
 def golden_arrays(name):
     z = np.load(os.path.join(GOLDEN, name + ".npz"))
     return {k: z[k] for k in z.files}
+
+
+@pytest.fixture(scope="module")
+def gpu_snapshots(snapshots):
+    """The parity snapshots resident on the GPU (FP32 and FP64 primitives)."""
+    import phoenix_b200 as P
+    out = {}
+    for name, (dump, grid, spec) in snapshots.items():
+        out[name] = P.Snapshot.load(dump, grid, nlevels=spec["nlevels"], sfc=spec["sfc"], f64_prims=True)
+    yield out
+    for s in out.values():
+        s.close()

@@ -20,16 +20,6 @@ TOL = {"fp64": dict(flux=1e-9, l1=1e-8), "fp32": dict(flux=1e-4, pol=1e-3, l1=1e
        "mixed": dict(flux=1e-4, pol=1e-3, l1=1e-3)}
 
 
-@pytest.fixture(scope="module")
-def gpu_snapshots(snapshots):
-    out = {}
-    for name, (dump, grid, spec) in snapshots.items():
-        out[name] = P.Snapshot.load(dump, grid, nlevels=spec["nlevels"], sfc=spec["sfc"], f64_prims=True)
-    yield out
-    for s in out.values():
-        s.close()
-
-
 def render_case(snaps, name, precision, **over):
     kw = case_params(name)
     kw.update(over)

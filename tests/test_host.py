@@ -121,3 +121,28 @@ def test_make_params_rejects_unknown_keys(built):
         native.make_params(no_such_key=1)
     p = native.make_params(frequencies=[86e9, 230e9], precision="mixed", img=32)
     assert p.nfreqs == 2 and p.precision == native.PREC_MIXED and p.img_width == p.img_height == 32
+
+
+def test_ctypes_structs_match_the_header(tmp_path):
+    """Size and field offsets of every struct the Python binding mirrors, as gcc lays out include/phoenix_b200.h."""
+    import subprocess
+    structs = {"PhxRenderParams": native.PhxRenderParams, "PhxRenderInfo": native.PhxRenderInfo,
+               "PhxSnapshotDesc": native.PhxSnapshotDesc, "PhxReadOptions": native.PhxReadOptions,
+               "PhxFreqOut": native.PhxFreqOut, "PhxBatchItem": native.PhxBatchItem,
+               "PhxBatchOptions": native.PhxBatchOptions, "PhxBatchTuning": native.PhxBatchTuning}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "phoenix_b200.h"', "int main(void) {"]
+    for name, cls in structs.items():
+        lines.append(f'  printf("{name} size %zu\\n", sizeof({name}));')
+        for field, _ in cls._fields_:
+            lines.append(f'  printf("{name} {field} %zu\\n", offsetof({name}, {field}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.check_call(["gcc", "-I" + os.path.join(ROOT, "include"), str(src), "-o", str(exe)])
+    out = subprocess.check_output([str(exe)]).decode().split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for name, cls in structs.items():
+        assert got[(name, "size")] == C.sizeof(cls), name
+        for field, _ in cls._fields_:
+            assert got[(name, field)] == getattr(cls, field).offset, (name, field)
