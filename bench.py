@@ -321,6 +321,108 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
+# Serving workload: 4 resident snapshots (seeds 0-3, base grids 96x48x48 .. 256x128x128, 2-4 AMR levels, FP32
+# fields) and seeded Poisson request streams.
+SERVE = dict(
+    snapshots=[["--seed", "0", "--base", "96", "48", "48", "--nlevels", "2", "--nws", "0"],
+               ["--seed", "1", "--base", "128", "64", "64", "--nlevels", "3", "--nws", "0"],
+               ["--seed", "2", "--base", "192", "96", "96", "--nlevels", "3", "--nws", "0", "--refine", "3.5", "25",
+                "0.55"],
+               ["--seed", "3", "--base", "256", "128", "128", "--nlevels", "4", "--nws", "0", "--refine", "3.5", "15",
+                "0.4"]],
+    nlevels=[2, 3, 3, 4], seed=11, resolutions=(64, 128, 256, 512, 1024), freq=(86e9, 345e9), nfreq=(1, 4),
+    incl=(5.0, 175.0), m_unit=(1e17, 1e19), rates=(1, 2, 10, 50, 100, 200), requests=48, budget=150 << 30)
+
+
+def serve_requests(n, seed, cfg=SERVE):
+    """Seeded request list: snapshot, resolution, 1-4 frequencies, inclination, m_unit."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        nf = int(rng.integers(cfg["nfreq"][0], cfg["nfreq"][1] + 1))
+        fr = np.sort(np.exp(rng.uniform(np.log(cfg["freq"][0]), np.log(cfg["freq"][1]), nf)))
+        out.append(dict(snapshot=int(rng.integers(0, len(cfg["snapshots"]))),
+                        img=int(rng.choice(cfg["resolutions"])), frequencies=[float(f) for f in fr],
+                        inclination=float(rng.uniform(*cfg["incl"])),
+                        m_unit=float(np.exp(rng.uniform(np.log(cfg["m_unit"][0]), np.log(cfg["m_unit"][1]))))))
+    return out
+
+
+def run_serve(args):
+    """Config 5: Poisson request streams at several rates through the continuous-batching server; p50/p99 latency
+    (submission to result in host memory), throughput, and latency over the same request's isolated latency (the
+    request alone on the server).  Prints one JSON line."""
+    import threading
+
+    import phoenix_b200 as P
+    snaps = []
+    t0 = time.time()
+    for g, nl in zip(SERVE["snapshots"], SERVE["nlevels"]):
+        dump, grid = generated_snapshot(g)
+        snaps.append(P.Snapshot.load(dump, grid, nlevels=nl))
+    setup_s = time.time() - t0
+    reqs = serve_requests(args.requests or SERVE["requests"], SERVE["seed"])
+    params = [P.make_params(precision="fp32", img=r["img"], frequencies=r["frequencies"],
+                            inclination=r["inclination"], m_unit=r["m_unit"]) for r in reqs]
+    line = {"workload": "serve", "metric": "latency p50/p99 and rays/s", "n_gpus": 1, "data": "synthetic",
+            "config": {"snapshots": [" ".join(g) for g in SERVE["snapshots"]],
+                       "snapshot_bytes": [s.nbytes() for s in snaps], "requests": len(reqs),
+                       "request_seed": SERVE["seed"], "resolutions": list(SERVE["resolutions"]),
+                       "precision": "fp32", "budget_bytes": SERVE["budget"]},
+            "setup_s": setup_s}
+    with P.Server(snaps, "fp32", memory_budget=SERVE["budget"]) as srv:
+        # isolated latency of every request (alone on the server), after one warm-up request
+        w = srv.submit(0, params[0])
+        srv.wait(w)
+        srv.result(w)
+        iso = []
+        for r, p in zip(reqs, params):
+            rid = srv.submit(r["snapshot"], p)
+            srv.wait(rid)
+            iso.append(srv.result(rid)[1]["done_s"])
+        iso = np.array(iso)
+        rays = np.array([p.img_width * p.img_height for p in params], dtype=np.float64)
+        line["isolated"] = {"total_s": float(iso.sum()), "p50_s": float(np.median(iso)),
+                            "p99_s": float(np.percentile(iso, 99)), "rays_per_s": float(rays.sum() / iso.sum())}
+        runs = []
+        for rate in (args.rates or SERVE["rates"]):
+            rng = np.random.default_rng(SERVE["seed"] + int(rate))
+            arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
+            ids = [None] * len(reqs)
+            start = time.perf_counter()
+
+            def submitter():
+                for k, (r, p) in enumerate(zip(reqs, params)):
+                    delay = arrivals[k] - (time.perf_counter() - start)
+                    if delay > 0:
+                        time.sleep(delay)
+                    ids[k] = srv.submit(r["snapshot"], p)
+
+            th = threading.Thread(target=submitter)
+            th.start()
+            th.join()
+            lat, steps = [], 0
+            for rid in ids:
+                srv.wait(rid)
+                _, t = srv.result(rid)
+                lat.append(t["done_s"])
+                steps += t["steps"]
+            span = time.perf_counter() - start
+            lat = np.array(lat)
+            ratio = lat / iso
+            runs.append({"rate_per_s": rate, "offered_rays_per_s": float(rays.sum() / arrivals[-1]),
+                         "makespan_s": span, "rays_per_s": float(rays.sum() / span),
+                         "ray_steps_per_s": steps / span, "requests_per_s": len(reqs) / span,
+                         "p50_s": float(np.median(lat)), "p99_s": float(np.percentile(lat, 99)),
+                         "ratio_to_isolated_p50": float(np.median(ratio)),
+                         "ratio_to_isolated_p99": float(np.percentile(ratio, 99))})
+        line["runs"] = runs
+        line["server"] = srv.stats()
+    for s in snaps:
+        s.close()
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -332,14 +434,19 @@ def main():
     ap.add_argument("--period", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="plain", choices=["plain", "batch"],
-                    help="plain: the headline single-image path (default); batch: the 128-image sweep")
+    ap.add_argument("--workload", default="plain", choices=["plain", "batch", "serve"],
+                    help="plain: the headline single-image path (default); batch: the 128-image sweep; "
+                         "serve: Poisson request streams through the server")
+    ap.add_argument("--requests", type=int, default=0, help="serve: requests per stream")
+    ap.add_argument("--rates", type=float, nargs="*", default=None, help="serve: arrival rates [1/s]")
     ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "serve":
+        return run_serve(args)
 
     import torch
     import torch.distributed as dist

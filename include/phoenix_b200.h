@@ -93,12 +93,12 @@ typedef struct {
   double m_unit, r_low, r_high, beta_c, sigma_cut, thetae_min, thetae_max, rt_outer;
   /* this library */
   int32_t precision;   /* PHX_PREC_* */
-  double r_fp64;       /* mixed: FP64 RK4 inside r < r_fp64 * r_horizon (<= 0: default 1.5) */
+  double r_fp64;       /* mixed: FP64 RK4 inside r < r_fp64 * r_horizon (<= 0: default 3, the photon-orbit region) */
   double tau_fp64;     /* mixed: FP64 segment operator where h max|K| exceeds this (<= 0: default 0.1) */
   int32_t block;       /* threads per block, 0 = default */
   int32_t period;      /* march passes between lane refills, 0 = default (32) */
   int32_t blocks_per_sm; /* register-cap variant: resident 128-thread blocks per SM the kernel is compiled for
-                            (1: up to 255 registers, 3: 168, 4: 128); 0 = default (3) */
+                            (1: up to 255 registers, 3: 168, 4: 128); 0 = default (3; mixed: 1) */
 } PhxRenderParams;
 
 /* What a render reports (a superset of the reference's device::Info, src/device/kernel.cuh:23-30). */
@@ -229,6 +229,70 @@ int phx_batch_device_result(PhxBatch* b, int32_t item, PhxFreqOut** d_res);
 int phx_batch_tuning(const PhxBatch* b, PhxBatchTuning* t);
 
 void phx_batch_destroy(PhxBatch* b);
+
+/* ---- Serving: continuous batching of render requests ----
+ * No reference counterpart (the reference renders one configured image per process run, src/main.cpp:120-205).  A
+ * server keeps snapshots resident, admits requests first-in first-out by device memory (a result arena inside
+ * memory_budget), and merges each admitted request's rays into one running queue kernel while earlier requests are
+ * still on the GPU.  Each request's result equals what phx_render returns for it, to the rounding of the separately
+ * compiled kernel, whatever else runs beside it.  The API is thread-safe; all CUDA work runs on the server's own
+ * scheduler thread. */
+typedef struct PhxServer PhxServer;
+
+enum { PHX_REQ_QUEUED = 0, PHX_REQ_RUNNING = 1, PHX_REQ_DONE = 2, PHX_REQ_FAILED = 3 };
+
+typedef struct {
+  int64_t memory_budget;  /* device bytes for snapshots, queue tables and the result arena (default 150 GiB) */
+  int64_t arena_bytes;    /* results + job lists of requests in flight, 0 = min(what the budget leaves, 16 GiB) */
+  int32_t precision;      /* PHX_PREC_*, shared by every request */
+  int32_t max_freqs;      /* frequency slots per request (1 or 4; FP32 also up to 32), default 4 */
+  int32_t tile_rays;      /* rays per queue tile, default 32 */
+  int32_t period;         /* march passes between lane refills, default 32 */
+  int32_t blocks_per_sm;  /* register-cap variant, default 3 */
+  int32_t max_items;      /* requests per run of the kernel before the queue is recycled, default 4096 */
+  int64_t max_tiles;      /* tiles per run of the kernel, a power of two, default 2^22 */
+  int32_t idle_ns;        /* sleep of an idle warp between polls of the queue, default 2000 */
+  int64_t idle_limit;     /* polls after which an idle warp stops waiting and the kernel leaves, default 5e6 */
+  double linger_ms;       /* idle time after which the scheduler stops the kernel, default 20 */
+  int32_t poll_us;        /* scheduler polling interval, default 50 */
+} PhxServerOptions;
+
+typedef struct {
+  double submitted_s;     /* submission time since the server was created */
+  double admitted_s;      /* seconds from submission to publication into the queue */
+  double done_s;          /* seconds from submission to the result being back in host memory */
+  int64_t rays, steps, nplasma, bad;
+} PhxRequestTiming;
+
+typedef struct {
+  int64_t submitted, completed, inflight, pending, generations;
+  int64_t rays, steps;
+  int64_t snapshot_bytes, table_bytes, arena_bytes, arena_used, job_table_bytes;
+  int32_t grid, regs;
+} PhxServerStats;
+
+void phx_default_server_options(PhxServerOptions* o);
+
+/* Starts a server over nsnaps resident snapshots (not owned: keep them alive until phx_server_destroy). */
+int phx_server_create(PhxSnapshot* const* snaps, int32_t nsnaps, const PhxServerOptions* opt, PhxServer** out);
+
+/* Queues a render of snapshot `snapshot` (index into the creation list); returns at once with its id. */
+int phx_server_submit(PhxServer* s, int32_t snapshot, const PhxRenderParams* p, int64_t* request);
+
+/* Current state (PHX_REQ_*) of a request. */
+int phx_server_poll(PhxServer* s, int64_t request, int32_t* state);
+
+/* Waits until the request is done or failed, at most timeout_s seconds (<= 0: no limit); PHX_E_TIMEOUT if not done. */
+int phx_server_wait(PhxServer* s, int64_t request, double timeout_s, int32_t* state);
+
+/* A finished request's records (img_width * img_height * nfreqs, index (i * img_height + j) * nfreqs + f) and
+ * timing; releases the request (its id is unknown afterwards). */
+int phx_server_result(PhxServer* s, int64_t request, PhxFreqOut* res, PhxRequestTiming* timing);
+
+int phx_server_stats(PhxServer* s, PhxServerStats* st);
+
+/* Finishes the requests in flight, stops the kernel and frees the server's device memory. */
+void phx_server_destroy(PhxServer* s);
 
 /* Writes a render's outputs the way PHOENIX's write_output does (src/main.cpp:52-86, src/host/io/output.hpp):
  * `image` = "hdf5" -> outdir/img_data.h5 (RAPTOR block layout, block_size pixels per side; if it cannot be written the

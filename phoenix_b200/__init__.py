@@ -16,7 +16,7 @@ from . import native
 from .native import (CTR, NUM_COUNTERS, PREC_FP32, PREC_FP64, PREC_MIXED, PhxError, PhxRenderInfo, make_params,
                      schedule_morton, write_output)
 
-__all__ = ["Snapshot", "Batch", "make_params", "schedule_morton", "write_output", "flux", "pixel_solid_angle", "PhxError", "PREC_FP32",
+__all__ = ["Snapshot", "Batch", "Server", "make_params", "schedule_morton", "write_output", "flux", "pixel_solid_angle", "PhxError", "PREC_FP32",
            "PREC_FP64", "PREC_MIXED", "CTR", "NUM_COUNTERS"]
 
 G_GRAV, M_SUN, C_LIGHT, KPC, JANSKY = 6.674e-8, 1.989e33, 2.99792458e10, 3.086e21, 1e23
@@ -168,6 +168,73 @@ class Batch:
     def close(self):
         if self._h and self._h.value:
             native.lib().phx_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching render server over resident snapshots (one precision; thread-safe).  Requests are
+    admitted by device memory and merged into one running queue kernel while earlier requests are on the GPU."""
+
+    def __init__(self, snapshots, precision="fp32", **opts):
+        L = native.lib()
+        o = native.PhxServerOptions()
+        L.phx_default_server_options(C.byref(o))
+        o.precision = native.PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        for k, v in opts.items():
+            if not hasattr(o, k):
+                raise KeyError(f"unknown server option {k}")
+            setattr(o, k, v)
+        self._snaps = list(snapshots)
+        arr = (C.c_void_p * len(self._snaps))(*[sn.handle.value for sn in self._snaps])
+        h = C.c_void_p()
+        native.check(L.phx_server_create(arr, len(self._snaps), C.byref(o), C.byref(h)))
+        self._h = h
+        self._params = {}
+
+    def submit(self, snapshot: int, params) -> int:
+        rid = C.c_int64()
+        native.check(native.lib().phx_server_submit(self._h, snapshot, C.byref(params), C.byref(rid)))
+        self._params[rid.value] = params
+        return rid.value
+
+    def poll(self, rid: int) -> int:
+        st = C.c_int32()
+        native.check(native.lib().phx_server_poll(self._h, rid, C.byref(st)))
+        return st.value
+
+    def wait(self, rid: int, timeout: float = 0.0) -> int:
+        st = C.c_int32()
+        native.check(native.lib().phx_server_wait(self._h, rid, timeout, C.byref(st)))
+        return st.value
+
+    def result(self, rid: int):
+        """(res[img_width, img_height, nfreqs, 6], timing dict) of a finished request; releases it."""
+        p = self._params.pop(rid)
+        res = np.zeros((p.img_width, p.img_height, p.nfreqs, 6), dtype=np.float64)
+        t = native.PhxRequestTiming()
+        native.check(native.lib().phx_server_result(self._h, rid, res.ctypes.data, C.byref(t)))
+        return res, t.as_dict()
+
+    def stats(self) -> dict:
+        st = native.PhxServerStats()
+        native.check(native.lib().phx_server_stats(self._h, C.byref(st)))
+        return st.as_dict()
+
+    def close(self):
+        if self._h and self._h.value:
+            native.lib().phx_server_destroy(self._h)
             self._h = C.c_void_p()
 
     def __enter__(self):

@@ -10,7 +10,7 @@
 //   FP32   float everywhere after the FP64 camera set-up; compensated (hi, lo) geodesic state with south-pole
 //          folding; deviation-form transfer operator.
 //   FP64   double everywhere.
-//   Mixed  FP32 bulk plus FP64 islands: RK4 steps inside r < r_fp64 (default 1.5 r_horizon), the null-condition
+//   Mixed  FP32 bulk plus FP64 islands: RK4 steps inside r < r_fp64 (default 3 r_horizon), the null-condition
 //          renormalisation of each sample's wave vector, the segment operator where h max|K| > tau_fp64 (large
 //          optical / Faraday depth per segment), Kahan summation of the Stokes vector, and the placement of samples
 //          in leaves and cells (the compensated FP32 position widened to FP64 against FP64 leaf geometry).  The last
@@ -203,10 +203,12 @@ struct Ray {
         ctr.scans += scanned;
       }
       if (ig == -1) return;
-      double qd[kNPrim];
-      interp_prims<double, PT, true>(sd, ig, xd, qd);
-#pragma unroll
-      for (int v = 0; v < kNPrim; v++) q[v] = R(qd[v]);
+      // cell and weights from the FP64 position; the weighted sum of the FP32 primitives stays FP32
+      int c[3];
+      double dd[3];
+      cell_weights<double, PT, true>(sd, ig, xd, c, dd);
+      const R del[3] = {R(dd[0]), R(dd[1]), R(dd[2])};
+      gather_prims<R, PT>(s.prim, s.cells, s.nx, ig, c, del, q);
 #pragma unroll
       for (int i = 0; i < 4; i++) x[i] = R(xd[i]);
     } else {

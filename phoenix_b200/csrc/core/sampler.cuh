@@ -165,12 +165,11 @@ PHX_HD int find_leaf(const SnapView<R, PT>& s, const R x[4], bool* scanned) {
   return -1;
 }
 
-// Trilinear interpolation of the 8 primitives inside one leaf, weights measured from the block's lower corner and
-// clamped at the block faces (no ghost cells).
+// Cell and trilinear weights of point x inside one leaf: weights measured from the block's lower corner and clamped at
+// the block faces (no ghost cells).  c: the lower corner cell (clamped into the block), del: weights of the upper
+// corners.
 template <class R, class PT, bool kFloorBy1000>
-PHX_HD void interp_prims(const SnapView<R, PT>& s, int leaf, const R x[4], R q[kNPrim]) {
-  int c[3], ix[3];
-  R del[3];
+PHX_HD void cell_weights(const SnapView<R, PT>& s, int leaf, const R x[4], int c[3], R del[3]) {
 #pragma unroll
   for (int d = 0; d < 3; d++) {
     const R lb = ldg(s.lb + 3 * leaf + d), dx = ldg(s.dxc + 3 * leaf + d);
@@ -178,18 +177,24 @@ PHX_HD void interp_prims(const SnapView<R, PT>& s, int leaf, const R x[4], R q[k
     c[d] = (int)u;
     if (c[d] >= s.nx[d]) c[d] = s.nx[d] - 1;
     if (c[d] < 0) c[d] = 0;  // unreachable for finite points of the leaf; keeps every gather inside the block
-    ix[d] = kFloorBy1000 ? (int)(u + R(1000)) - 1000 : (int)floor_t(u);
-    del[d] = (ix[d] < 0) ? R(0) : (ix[d] > s.nx[d] - 2) ? R(1) : (x[1 + d] - (R(ix[d]) * dx + lb)) / dx;
+    const int ix = kFloorBy1000 ? (int)(u + R(1000)) - 1000 : (int)floor_t(u);
+    del[d] = (ix < 0) ? R(0) : (ix > s.nx[d] - 2) ? R(1) : (x[1 + d] - (R(ix) * dx + lb)) / dx;
   }
-  const int nx0 = s.nx[0], nx01 = s.nx[0] * s.nx[1];
-  const int cip = c[0] + 1 < s.nx[0] ? c[0] + 1 : c[0];
-  const int cjp = c[1] + 1 < s.nx[1] ? c[1] + 1 : c[1];
-  const int ckp = c[2] + 1 < s.nx[2] ? c[2] + 1 : c[2];
+}
+
+// Weighted sum of the 8 primitives over the 2x2x2 corners from cell c (corners past the block's last cell reuse it).
+template <class R, class PT>
+PHX_HD void gather_prims(const PT* prim, int cells, const int nx[3], int leaf, const int c[3], const R del[3],
+                         R q[kNPrim]) {
+  const int nx0 = nx[0], nx01 = nx[0] * nx[1];
+  const int cip = c[0] + 1 < nx[0] ? c[0] + 1 : c[0];
+  const int cjp = c[1] + 1 < nx[1] ? c[1] + 1 : c[1];
+  const int ckp = c[2] + 1 < nx[2] ? c[2] + 1 : c[2];
   const R b1 = R(1) - del[0], b2 = R(1) - del[1], b3 = R(1) - del[2];
   const int ci[4] = {c[0], c[0], cip, cip};
   const int cj[4] = {c[1], cjp, c[1], cjp};
   const R wq[4] = {b1 * b2, b1 * del[1], del[0] * b2, del[0] * del[1]};
-  const PT* base = s.prim + (size_t)leaf * s.cells * kNPrim;
+  const PT* base = prim + (size_t)leaf * cells * kNPrim;
 #pragma unroll
   for (int a = 0; a < kNPrim; a++) q[a] = R(0);
 #pragma unroll
@@ -223,6 +228,15 @@ PHX_HD void interp_prims(const SnapView<R, PT>& s, int leaf, const R x[4], R q[k
       for (int a = 0; a < kNPrim; a++) q[a] += v[a] * w;
     }
   }
+}
+
+// Trilinear interpolation of the 8 primitives inside one leaf (sampler.hpp:211-291).
+template <class R, class PT, bool kFloorBy1000>
+PHX_HD void interp_prims(const SnapView<R, PT>& s, int leaf, const R x[4], R q[kNPrim]) {
+  int c[3];
+  R del[3];
+  cell_weights<R, PT, kFloorBy1000>(s, leaf, x, c, del);
+  gather_prims<R, PT>(s.prim, s.cells, s.nx, leaf, c, del, q);
 }
 
 // Fluid 4-velocity, magnetic 4-vector, |B| [G], n_e and Theta_e from the interpolated primitives; returns whether

@@ -50,8 +50,9 @@ cudaError_t launch_nf(const MarchArgs<typename Policy<M>::R, PT>& args, int sms,
         return launch_mb<M, PT, NF, 3>(args, sms, stream, shape);
       case 4:
         return launch_mb<M, PT, NF, 4>(args, sms, stream, shape);
-      default:  // measured on B200: 3 resident blocks (168 registers) for one and for four slots
-        return launch_mb<M, PT, NF, 3>(args, sms, stream, shape);
+      default:  // measured on B200: FP32 3 resident blocks (168 registers); mixed uncapped (it spills at 168)
+        if constexpr (M == Mode::kMixed) return launch_mb<M, PT, NF, 1>(args, sms, stream, shape);
+        else return launch_mb<M, PT, NF, 3>(args, sms, stream, shape);
     }
   }
 }

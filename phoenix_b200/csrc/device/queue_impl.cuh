@@ -35,14 +35,15 @@ cudaError_t launch_queue_mb(const QueueArgs<typename Policy<M>::R, PT>& args, in
 }
 
 // Register-cap variants as for the single-image kernel: FP32 is compiled for 1, 3 and 4 resident 128-thread blocks
-// per SM with one and four frequency slots; mixed for 3; FP64 and 32 slots uncapped.
+// per SM with one and four frequency slots; mixed for 1 and 3; FP64 and 32 slots uncapped.
 template <Mode M, class PT, int NF>
 cudaError_t launch_queue_nf(const QueueArgs<typename Policy<M>::R, PT>& args, int sms, QueueShape q,
                             long long max_rays, cudaStream_t stream, LaunchShape* shape) {
   if constexpr (M == Mode::kFP64 || NF > 4) {
     return launch_queue_mb<M, PT, NF, 1>(args, sms, q.period, max_rays, stream, shape);
   } else if constexpr (M == Mode::kMixed) {
-    return launch_queue_mb<M, PT, NF, 3>(args, sms, q.period, max_rays, stream, shape);
+    if (q.blocks_per_sm == 3) return launch_queue_mb<M, PT, NF, 3>(args, sms, q.period, max_rays, stream, shape);
+    return launch_queue_mb<M, PT, NF, 1>(args, sms, q.period, max_rays, stream, shape);
   } else {
     switch (q.blocks_per_sm) {
       case 1:

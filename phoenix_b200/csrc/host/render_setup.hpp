@@ -66,7 +66,7 @@ RenderConsts<R> make_consts(const PhxRenderParams& p, double a, double hslope) {
   rc.rt_outer = R(p.rt_outer);
   rc.step_tiny = sizeof(R) == 4 ? R(1e-30) : R(1e-160);
   rc.step_big = sizeof(R) == 4 ? R(1e30) : R(1e100);
-  rc.r_fp64 = R((p.r_fp64 > 0.0 ? p.r_fp64 : 1.5) * r_h);
+  rc.r_fp64 = R((p.r_fp64 > 0.0 ? p.r_fp64 : 3.0) * r_h);
   rc.tau_fp64 = R(p.tau_fp64 > 0.0 ? p.tau_fp64 : 0.1);
   rc.pv.Ne = R(u.Ne);
   rc.pv.Bu = R(u.B);

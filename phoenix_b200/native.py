@@ -27,7 +27,10 @@ CTR = dict(queue=0, steps=1, nplasma=2, bad=3, scans=4, fp64_steps=5, fp64_ops=6
 EXPORTS = ["phx_default_params", "phx_snapshot_create", "phx_snapshot_load", "phx_snapshot_destroy",
            "phx_bhac_read", "phx_bhac_describe", "phx_bhac_free", "phx_snapshot_bytes", "phx_schedule_morton", "phx_render", "phx_render_async", "phx_render_noalloc", "phx_write_output", "phx_last_error",
            "phx_version", "phx_default_batch_options", "phx_batch_create", "phx_batch_launch", "phx_batch_run",
-           "phx_batch_result", "phx_batch_device_result", "phx_batch_tuning", "phx_batch_destroy"]
+           "phx_batch_result", "phx_batch_device_result", "phx_batch_tuning", "phx_batch_destroy",
+           "phx_default_server_options", "phx_server_create", "phx_server_submit", "phx_server_poll",
+           "phx_server_wait", "phx_server_result", "phx_server_stats", "phx_server_destroy"]
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
 TUNE_MAX_CANDIDATES = 16
 
 
@@ -104,6 +107,32 @@ class PhxBatchTuning(C.Structure):
         return d
 
 
+class PhxServerOptions(C.Structure):
+    _fields_ = [
+        ("memory_budget", C.c_int64), ("arena_bytes", C.c_int64), ("precision", C.c_int32), ("max_freqs", C.c_int32),
+        ("tile_rays", C.c_int32), ("period", C.c_int32), ("blocks_per_sm", C.c_int32), ("max_items", C.c_int32),
+        ("max_tiles", C.c_int64), ("idle_ns", C.c_int32), ("idle_limit", C.c_int64), ("linger_ms", C.c_double),
+        ("poll_us", C.c_int32),
+    ]
+
+
+class PhxRequestTiming(C.Structure):
+    _fields_ = [("submitted_s", C.c_double), ("admitted_s", C.c_double), ("done_s", C.c_double),
+                ("rays", C.c_int64), ("steps", C.c_int64), ("nplasma", C.c_int64), ("bad", C.c_int64)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class PhxServerStats(C.Structure):
+    _fields_ = [(n, C.c_int64) for n in ("submitted", "completed", "inflight", "pending", "generations", "rays",
+                                         "steps", "snapshot_bytes", "table_bytes", "arena_bytes", "arena_used",
+                                         "job_table_bytes")] + [("grid", C.c_int32), ("regs", C.c_int32)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 class PhxError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"phoenix_b200 error {code}: {msg}")
@@ -153,6 +182,19 @@ def lib():
     L.phx_batch_tuning.argtypes = [C.c_void_p, P(PhxBatchTuning)]
     L.phx_batch_destroy.argtypes = [C.c_void_p]
     L.phx_batch_destroy.restype = None
+    L.phx_default_server_options.argtypes = [P(PhxServerOptions)]
+    L.phx_default_server_options.restype = None
+    L.phx_server_create.argtypes = [C.c_void_p, C.c_int32, P(PhxServerOptions), P(C.c_void_p)]
+    L.phx_server_submit.argtypes = [C.c_void_p, C.c_int32, P(PhxRenderParams), P(C.c_int64)]
+    L.phx_server_poll.argtypes = [C.c_void_p, C.c_int64, P(C.c_int32)]
+    L.phx_server_wait.argtypes = [C.c_void_p, C.c_int64, C.c_double, P(C.c_int32)]
+    L.phx_server_result.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, P(PhxRequestTiming)]
+    L.phx_server_stats.argtypes = [C.c_void_p, P(PhxServerStats)]
+    L.phx_server_destroy.argtypes = [C.c_void_p]
+    L.phx_server_destroy.restype = None
+    for name in ("phx_server_create", "phx_server_submit", "phx_server_poll", "phx_server_wait", "phx_server_result",
+                 "phx_server_stats"):
+        getattr(L, name).restype = C.c_int
     for name in ("phx_snapshot_create", "phx_snapshot_load", "phx_bhac_read", "phx_bhac_describe", "phx_schedule_morton",
                  "phx_render", "phx_render_async", "phx_render_noalloc", "phx_batch_create", "phx_batch_launch",
                  "phx_batch_run", "phx_batch_result", "phx_batch_device_result", "phx_batch_tuning"):

@@ -129,7 +129,9 @@ def test_ctypes_structs_match_the_header(tmp_path):
     structs = {"PhxRenderParams": native.PhxRenderParams, "PhxRenderInfo": native.PhxRenderInfo,
                "PhxSnapshotDesc": native.PhxSnapshotDesc, "PhxReadOptions": native.PhxReadOptions,
                "PhxFreqOut": native.PhxFreqOut, "PhxBatchItem": native.PhxBatchItem,
-               "PhxBatchOptions": native.PhxBatchOptions, "PhxBatchTuning": native.PhxBatchTuning}
+               "PhxBatchOptions": native.PhxBatchOptions, "PhxBatchTuning": native.PhxBatchTuning,
+               "PhxServerOptions": native.PhxServerOptions, "PhxRequestTiming": native.PhxRequestTiming,
+               "PhxServerStats": native.PhxServerStats}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "phoenix_b200.h"', "int main(void) {"]
     for name, cls in structs.items():
         lines.append(f'  printf("{name} size %zu\\n", sizeof({name}));')
