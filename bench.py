@@ -29,6 +29,7 @@ sys.path.insert(0, ROOT)
 
 GEN = os.path.join(ROOT, "phoenix_b200", "_build", "phx_gen_snapshot")
 REF_CPU = os.path.join(ROOT, "oracle", "_ref", "ref_render_fp32")
+REF_GPU = os.path.join(ROOT, "oracle", "_ref", "ref_gpu_fp32")
 
 WORKLOAD = dict(base=(192, 96, 96), nlevels=3, refine=(3.5, 25.0, 0.55), seed=0, img=512,
                 inclinations=(10.0, 60.0, 163.0), frequency=230e9, m_unit=1.2e18)
@@ -423,12 +424,56 @@ def run_serve(args):
     print(json.dumps(line), flush=True)
 
 
+def run_reference_gpu(args):
+    """The reference's own CUDA kernel (src/device/kernel.cu built for sm_100a from its sources, FP32, one frequency
+    slot, 128 threads x 3 blocks/SM as its CMake defaults) on the plain-path workload, timed by its own CUDA events
+    (device::Info.kernel_s: the kernel launches only, not its per-call model upload)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    if not os.path.exists(REF_GPU):
+        print(json.dumps({"impl": "reference_gpu", "unavailable": "oracle/_ref/ref_gpu_fp32 was not built "
+                                                                   "(the reference tree is needed to build it)"}))
+        return
+    from tests.golden.cases import write_config
+    w = dict(WORKLOAD)
+    w["img"] = args.img
+    dump, grid = snapshot_files(w)
+    K, W = max(1, args.steps), max(0, args.warmup)
+    with tempfile.TemporaryDirectory() as tmp:
+        case = dict(snapshot="cfg1", inclination=w["inclinations"][0], img_width=w["img"], img_height=w["img"],
+                    frequencies=[w["frequency"]], m_unit=w["m_unit"])
+        cfg = os.path.join(tmp, "c.toml")
+        write_config(cfg, case, dump, grid, tmp)
+        with open(cfg) as f:
+            text = f.read().replace("nlevels = 3", f"nlevels = {w['nlevels']}")
+        with open(cfg, "w") as f:
+            f.write(text)
+        out = subprocess.check_output([REF_GPU, cfg, "--inclinations", ",".join(str(i) for i in w["inclinations"]),
+                                       "--repeat", str(W + K)])
+    passes = [json.loads(l) for l in out.decode().splitlines() if l.strip().startswith("{")][W:]
+    steps = sum(p["steps"] for p in passes)
+    secs = sum(p["kernel_s"] for p in passes)
+    value = steps / secs
+    line = {"metric": "ray-steps/s", "value": value, "unit": "ray-steps/s", "n_gpus": 1, "steps": K, "warmup": W,
+            "ms_per_step": 1e3 * secs / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic", "impl": "reference_gpu",
+            "config": {"workload": "plain GPU path: 192x96x96 base grid, 8^3 blocks, 3 AMR levels (15.6M cells), "
+                                   f"3 x {w['img']}^2 images at 10/60/163 deg, 230 GHz, m_unit 1.2e18",
+                       "kernel": "reference src/device/kernel.cu k_render, FP32, PHX_MAX_FREQS=1, 128 x 3 blocks/SM",
+                       "timing": "the reference's own CUDA events around its launches (device::Info.kernel_s)"},
+            "regs": passes[-1]["regs"], "local_bytes": passes[-1]["local_bytes"],
+            "upload_s_per_step": sum(p["upload_s"] for p in passes) / K,
+            "ray_steps_per_step": steps / K}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference_gpu"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64", "mixed"])
     ap.add_argument("--img", type=int, default=WORKLOAD["img"], help="image side (profiling runs use smaller)")
     ap.add_argument("--period", type=int, default=0)
@@ -443,6 +488,8 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.impl == "reference_gpu":
+        return run_reference_gpu(args)
     if args.workload == "batch":
         return run_batch(args)
     if args.workload == "serve":
