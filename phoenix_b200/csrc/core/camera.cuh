@@ -103,18 +103,20 @@ template <class R>
 PHX_HD void observer_axes(const Cov<R>& g, R sqrtg, const R k[4], const R U[4], const R b[4], R perp[4], R para[4],
                           R* omega_out) {
   const R omega = -dot(g, k, U);
+  const R iomega = R(1) / omega;
   R eK[4];
-  for (int i = 0; i < 4; i++) eK[i] = k[i] / omega - U[i];
+  for (int i = 0; i < 4; i++) eK[i] = k[i] * iomega - U[i];
   const R Beta = dot(g, U, b);
-  const R Cc = dot(g, k, b) / omega - Beta;
+  const R Cc = dot(g, k, b) * iomega - Beta;
   const R b2 = dot(g, b, b);
   const R Nc = sqrt_t(b2 + Beta * Beta - Cc * Cc);
-  for (int i = 0; i < 4; i++) para[i] = (b[i] + Beta * U[i] - Cc * eK[i]) / Nc;
+  const R iNc = R(1) / Nc;
+  for (int i = 0; i < 4; i++) para[i] = (b[i] + Beta * U[i] - Cc * eK[i]) * iNc;
   R Ud[4], kd[4], bd[4];
   symv(g, U, Ud);
   symv(g, k, kd);
   symv(g, b, bd);
-  const R s = R(-1) / (sqrtg * omega * Nc);
+  const R s = -iomega * iNc / sqrtg;
   // generalized cross product: perp^i = (-1)^i det[U, k, b] over the three columns other than i
   const R m01 = kd[0] * bd[1] - kd[1] * bd[0], m02 = kd[0] * bd[2] - kd[2] * bd[0], m03 = kd[0] * bd[3] - kd[3] * bd[0];
   const R m12 = kd[1] * bd[2] - kd[2] * bd[1], m13 = kd[1] * bd[3] - kd[3] * bd[1], m23 = kd[2] * bd[3] - kd[3] * bd[2];

@@ -10,9 +10,11 @@
 #if defined(__CUDACC__)
 #define PHX_HD __host__ __device__ __forceinline__
 #define PHX_D __device__ __forceinline__
+#define PHX_HD_OUTLINE __host__ __device__ __noinline__
 #else
 #define PHX_HD inline
 #define PHX_D inline
+#define PHX_HD_OUTLINE __attribute__((noinline))
 #endif
 
 namespace phx {

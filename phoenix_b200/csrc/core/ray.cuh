@@ -56,12 +56,33 @@ struct RenderConsts {
   int32_t W, H, nfreqs, max_steps, max_order;
   double fov_x, fov_y, cos_pa, sin_pa;
   CameraSpec cam;
-  R stepsize, r_out, cut_in, rt_outer;
+  R stepsize, inv_stepsize, r_out, cut_in, rt_outer;
   R step_tiny, step_big;
   R r_fp64, tau_fp64;
   PlasmaView<R> pv;
   R freq[kMaxFreqs], hconst[kMaxFreqs], jscale[kMaxFreqs];
 };
+
+// The camera set-up of one pixel in FP64: initial photon state (x, k), polarization vector F1 and the sign of the
+// impact parameter beta.
+struct RayStart {
+  double ph[8], F1[4];
+  int bsign;
+};
+
+// Kept out of line: it runs once per ray, and its FP64 code (impact parameters, the Newton solve for x2, the camera
+// tetrad) inlined into the march loop would crowd the loop's instruction cache and register allocation.
+template <class R>
+PHX_HD_OUTLINE RayStart ray_start(const RenderConsts<R>& rc, R a, R hs, int32_t pixel) {
+  RayStart st;
+  const int i = pixel / rc.H, j = pixel % rc.H;
+  double alpha, beta;
+  pixel_impact(i, j, rc.W, rc.H, rc.fov_x, rc.fov_y, rc.cos_pa, rc.sin_pa, &alpha, &beta);
+  camera_photon(rc.cam, alpha, beta, st.ph);
+  camera_pol<R>(a, hs, st.ph, st.F1);
+  st.bsign = beta < 0.0 ? -1 : (beta > 0.0 ? 1 : 0);
+  return st;
+}
 
 // Diagnostic counters a ray adds to.
 struct RayCounters {
@@ -81,24 +102,23 @@ struct Ray {
   int steps, turns, bsign, nplasma, bad;
   R thdot_prev, dl_prev;
   int32_t pix;
+  int leaf;     // leaf of the last step-size lookup (-1: none), tested before the leaf map
+  R idxc[3];    // its inverse cell sizes
   StokesAcc<R, kMixed> acc[NF];
 
   PHX_HD void init(const SnapView<R, PT>& s, const RenderConsts<R>& rc, int32_t pixel) {
     pix = pixel;
-    const int i = pixel / rc.H, j = pixel % rc.H;
-    double alpha, beta;
-    pixel_impact(i, j, rc.W, rc.H, rc.fov_x, rc.fov_y, rc.cos_pa, rc.sin_pa, &alpha, &beta);
-    double ph[8], F1[4];
-    camera_photon(rc.cam, alpha, beta, ph);
-    camera_pol<R>(s.a, s.hs, ph, F1);
-    geo_init<R, kComp>(geo, ph, F1);
+    const RayStart st = ray_start<R>(rc, s.a, s.hs, pixel);
+    geo_init<R, kComp>(geo, st.ph, st.F1);
 #pragma unroll
     for (int f = 0; f < NF; f++) acc[f].reset();
     pvalid = false;
     terminate = false;
     steps = turns = nplasma = bad = 0;
-    bsign = beta < 0.0 ? -1 : (beta > 0.0 ? 1 : 0);
+    bsign = st.bsign;
     thdot_prev = dl_prev = R(0);
+    leaf = -1;
+    idxc[0] = idxc[1] = idxc[2] = R(0);
   }
 
   // One pass of the march loop; false once the ray has ended (its pending sample has then been processed).
@@ -123,9 +143,20 @@ struct Ray {
       // the step-size cap and the sample's cache seed: FP32 in every FP32 mode (mixed re-checks the seed in FP64)
       R xw[4] = {cx[0], cx[1], cx[2], cx[3]};
       wrap_coords(xw);
-      bool scanned = false;
-      L = find_leaf(s, xw, &scanned);
-      ctr.scans += scanned;
+      // a ray stays tens of steps in one leaf: test the last one before the map (the leaves tile the domain, so a
+      // point inside it has no other leaf)
+      if (leaf >= 0 && inside_leaf(s, leaf, xw, leaf_nudge(xw))) {
+        L = leaf;
+      } else {
+        bool scanned = false;
+        L = find_leaf(s, xw, &scanned);
+        ctr.scans += scanned;
+        if (L >= 0 && L != leaf) {
+#pragma unroll
+          for (int d = 0; d < 3; d++) idxc[d] = R(1) / ldg(s.dxc + 3 * L + d);
+        }
+        leaf = L;
+      }
       if (need_leaf) right = (exp_t(xw[1]) < R(1) || outside_domain(s, xw)) ? -1 : L;
     }
     if (pend_plasma) process_sample(s, rc, right, ctr);
@@ -144,14 +175,20 @@ struct Ray {
     thdot_prev = ck[2];
     if ((bsign < 0 && turns > rc.max_order) || (bsign > 0 && turns > rc.max_order + 1)) terminate = true;
 
-    R dxcv[3];
     const bool cap = need_dxc && L >= 0;
-    if (cap) {
-#pragma unroll
-      for (int d = 0; d < 3; d++) dxcv[d] = ldg(s.dxc + 3 * L + d);
-    }
     const R x2 = pole_x2<R, kComp>(geo);
-    const R dl = step_size(rc.stepsize, x2, ck, cap ? dxcv : (const R*)nullptr, rc.step_tiny, rc.step_big);
+    R dl;
+    if constexpr (sizeof(R) == 4) {
+      dl = step_size_fast(rc.stepsize, rc.inv_stepsize, x2, ck, cap ? idxc : (const R*)nullptr, rc.step_tiny,
+                          rc.step_big);
+    } else {
+      R dxcv[3];
+      if (cap) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) dxcv[d] = ldg(s.dxc + 3 * L + d);
+      }
+      dl = step_size(rc.stepsize, x2, ck, cap ? dxcv : (const R*)nullptr, rc.step_tiny, rc.step_big);
+    }
     if constexpr (kMixed) {
       if (r < rc.r_fp64) {
         rk4_step_widened((double)s.a, (double)s.hs, geo, (double)dl);
@@ -246,8 +283,8 @@ struct Ray {
     R perp[4], para[4], omega;
     observer_axes(g, sqrt_neg_g(p), k, fl.U, fl.B, perp, para, &omega);
     const R C = dot(g, perp, pF), S = dot(g, para, pF);
-    const R nn = C * C + S * S;
-    const R c2 = (C * C - S * S) / nn, s2 = R(2) * C * S / nn;
+    const R inn = R(1) / (C * C + S * S);
+    const R c2 = (C * C - S * S) * inn, s2 = R(2) * C * S * inn;
     const R ratio = -kU;  // nu_plasma / nu_camera
     const SynchroSample<R> ss = synchro_sample(fl.theta_e, fl.n_e, fl.Bmag, sth, cth);
 #pragma unroll

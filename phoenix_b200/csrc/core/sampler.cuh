@@ -247,13 +247,16 @@ PHX_HD bool derive_fluid(const PlasmaView<R>& pv, R gam, R r, const Cov<R>& g, c
   const R smalll = R(1e-6);
   const R rho = q[kRho], uu = q[kUU];
   fl->n_e = rho * pv.Ne + smalll;
-  const R shift1 = u.t1 / (-u.tt);
-  const R alpha = R(1) / sqrt_t(-u.tt);
+  // lapse alpha = 1 / sqrt(-g^tt), shift^1 = alpha^2 g^t1; the divisions are folded into reciprocals
+  const R ialpha = sqrt_t(-u.tt);
+  const R alpha = R(1) / ialpha;
+  const R shift1 = u.t1 * alpha * alpha;
   const R gv1 = q[kU1], gv2 = q[kU2], gv3 = q[kU3];
   const R gvv = g.x11 * gv1 * gv1 + R(2) * g.x13 * gv1 * gv3 + g.x22 * gv2 * gv2 + g.x33 * gv3 * gv3;
   const R lfac = sqrt_t(gvv + R(1));
-  const R V1 = gv1 / lfac, V2 = gv2 / lfac, V3 = gv3 / lfac;
-  const R ut = lfac / alpha;
+  const R ilfac = R(1) / lfac;
+  const R V1 = gv1 * ilfac, V2 = gv2 * ilfac, V3 = gv3 * ilfac;
+  const R ut = lfac * ialpha;
   fl->U[0] = ut;
   fl->U[1] = V1 * lfac - shift1 * ut;
   fl->U[2] = V2 * lfac;
@@ -261,10 +264,10 @@ PHX_HD bool derive_fluid(const PlasmaView<R>& pv, R gam, R r, const Cov<R>& g, c
   const R Bp1 = q[kB1], Bp2 = q[kB2], Bp3 = q[kB3];
   // B^t = lfac (gamma_ij Bp^i V^j) / alpha
   const R BV = Bp1 * (g.x11 * V1 + g.x13 * V3) + Bp2 * (g.x22 * V2) + Bp3 * (g.x13 * V1 + g.x33 * V3);
-  fl->B[0] = lfac * BV / alpha;
-  fl->B[1] = (Bp1 + alpha * fl->B[0] * fl->U[1]) / lfac;
-  fl->B[2] = (Bp2 + alpha * fl->B[0] * fl->U[2]) / lfac;
-  fl->B[3] = (Bp3 + alpha * fl->B[0] * fl->U[3]) / lfac;
+  fl->B[0] = lfac * BV * ialpha;
+  fl->B[1] = (Bp1 + alpha * fl->B[0] * fl->U[1]) * ilfac;
+  fl->B[2] = (Bp2 + alpha * fl->B[0] * fl->U[2]) * ilfac;
+  fl->B[3] = (Bp3 + alpha * fl->B[0] * fl->U[3]) * ilfac;
   const R Bsq = fabs_t(dot(g, fl->B, fl->B)) + smalll;
   fl->Bmag = sqrt_t(Bsq) * pv.Bu;
   const R beta = uu * (gam - R(1)) / (R(0.5) * (Bsq + smalll));

@@ -60,6 +60,7 @@ RenderConsts<R> make_consts(const PhxRenderParams& p, double a, double hslope) {
   rc.cam.r_cam = p.r_cam;
   rc.cam.t_init = p.t_init;
   rc.stepsize = R(p.stepsize);
+  rc.inv_stepsize = R(1.0 / p.stepsize);
   const double r_h = 1.0 + std::sqrt(1.0 - a * a);
   rc.cut_in = R(r_h * (1.0 + p.horizon_margin));
   rc.r_out = R(1.1 * p.r_cam);
