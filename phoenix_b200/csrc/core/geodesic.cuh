@@ -115,8 +115,10 @@ PHX_HD void rk4_step(R a, R hs, GeoState<R>& g, R dt) {
   }
 }
 
-// FP64 RK4 step of an FP32 compensated state: the pair is widened to double, stepped, and split back.
-PHX_HD void rk4_step_widened(double a, double hs, GeoState<float>& g, double dt) {
+// FP64 RK4 step of an FP32 compensated state: the pair is widened to double, stepped, and split back.  Out of line
+// (state passed and returned by value): the mixed-precision island is a few percent of the steps, and its FP64 stage
+// body inlined beside the FP32 one would crowd the march loop's instruction cache.
+static PHX_HD_OUTLINE GeoState<float> rk4_step_widened_ool(double a, double hs, GeoState<float> g, double dt) {
   GeoState<double> w;
 #pragma unroll
   for (int i = 0; i < 12; i++) {
@@ -129,6 +131,11 @@ PHX_HD void rk4_step_widened(double a, double hs, GeoState<float>& g, double dt)
     g.hi[i] = (float)w.hi[i];
     g.lo[i] = (float)(w.hi[i] - (double)g.hi[i]);
   }
+  return g;
+}
+
+static PHX_HD void rk4_step_widened(double a, double hs, GeoState<float>& g, double dt) {
+  g = rk4_step_widened_ool(a, hs, g, dt);
 }
 
 // RAPTOR step size (negative: the ray runs backwards from the camera), capped by a quarter of the AMR cell.

@@ -148,6 +148,16 @@ PHX_HD bool inside_cached(const SnapView<R, PT>& s, int leaf, const R x[4]) {
   return in;
 }
 
+// Linear scan in leaf order: the first leaf whose half-open box holds the nudged point.  The rare fallback of
+// find_leaf, kept out of line so that it costs the march loop no instruction-cache space.
+template <class R, class PT>
+PHX_HD_OUTLINE int find_leaf_scan(const SnapView<R, PT>& s, R x1, R x2, R x3, R small) {
+  const R x[4] = {R(0), x1, x2, x3};
+  for (int leaf = 0; leaf < s.nleafs; leaf++)
+    if (inside_leaf(s, leaf, x, small)) return leaf;
+  return -1;
+}
+
 // Counts of the rare slow path, for diagnostics (incremented by the caller when `scanned` is set).
 template <class R, class PT>
 PHX_HD int find_leaf(const SnapView<R, PT>& s, const R x[4], bool* scanned) {
@@ -158,11 +168,8 @@ PHX_HD int find_leaf(const SnapView<R, PT>& s, const R x[4], bool* scanned) {
   if (cand < 0 && (x[1] < s.x_lo[1] - eps || x[1] > s.x_hi[1] + eps || x[2] < s.x_lo[2] - eps ||
                    x[2] > s.x_hi[2] + eps || x[3] < s.x_lo[3] - eps || x[3] > s.x_hi[3] + eps))
     return -1;
-  // linear scan in leaf order: the first leaf whose half-open box holds the nudged point
   *scanned = true;
-  for (int leaf = 0; leaf < s.nleafs; leaf++)
-    if (inside_leaf(s, leaf, x, small)) return leaf;
-  return -1;
+  return find_leaf_scan(s, x[1], x[2], x[3], small);
 }
 
 // Cell and trilinear weights of point x inside one leaf: weights measured from the block's lower corner and clamped at
@@ -173,12 +180,15 @@ PHX_HD void cell_weights(const SnapView<R, PT>& s, int leaf, const R x[4], int c
 #pragma unroll
   for (int d = 0; d < 3; d++) {
     const R lb = ldg(s.lb + 3 * leaf + d), dx = ldg(s.dxc + 3 * leaf + d);
-    const R u = (x[1 + d] - lb) / dx;
+    // FP32: one reciprocal per axis (rounding-level difference; the interpolant is continuous across cells)
+    const R idx = sizeof(R) == 4 ? R(1) / dx : R(0);
+    const R u = sizeof(R) == 4 ? (x[1 + d] - lb) * idx : (x[1 + d] - lb) / dx;
     c[d] = (int)u;
     if (c[d] >= s.nx[d]) c[d] = s.nx[d] - 1;
     if (c[d] < 0) c[d] = 0;  // unreachable for finite points of the leaf; keeps every gather inside the block
     const int ix = kFloorBy1000 ? (int)(u + R(1000)) - 1000 : (int)floor_t(u);
-    del[d] = (ix < 0) ? R(0) : (ix > s.nx[d] - 2) ? R(1) : (x[1 + d] - (R(ix) * dx + lb)) / dx;
+    const R off = x[1 + d] - (R(ix) * dx + lb);
+    del[d] = (ix < 0) ? R(0) : (ix > s.nx[d] - 2) ? R(1) : (sizeof(R) == 4 ? off * idx : off / dx);
   }
 }
 

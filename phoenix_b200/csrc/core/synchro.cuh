@@ -56,14 +56,27 @@ PHX_HD R hankel_sum(int nu, R x, R tol) {
   return sum;
 }
 
+template <class R>
+struct RatioPair {
+  R r10, r02;
+};
+
+// K1/K2 and K0/K2 from the Hankel series (x >= 30: Theta_e < 1/30), out of line: cool plasma is a minority of the
+// samples and its series loops would otherwise sit in the march loop's instruction stream.
+template <class R>
+PHX_HD_OUTLINE RatioPair<R> bessel_ratios_hankel(R x) {
+  const R tol = sizeof(R) == 4 ? R(1e-8) : R(1e-17);
+  const R s2 = hankel_sum(2, x, tol);
+  return {hankel_sum(1, x, tol) / s2, hankel_sum(0, x, tol) / s2};
+}
+
 // K1(x)/K2(x) and K0(x)/K2(x) for x >= 0.2 (x = 1/Theta_e; hotter plasma never calls this).
 template <class R>
 PHX_HD void bessel_ratios(R x, R* r10, R* r02) {
   if (x >= R(30)) {
-    const R tol = sizeof(R) == 4 ? R(1e-8) : R(1e-17);
-    const R s2 = hankel_sum(2, x, tol);
-    *r10 = hankel_sum(1, x, tol) / s2;
-    *r02 = hankel_sum(0, x, tol) / s2;
+    const RatioPair<R> rp = bessel_ratios_hankel(x);
+    *r10 = rp.r10;
+    *r02 = rp.r02;
     return;
   }
   const BesselPiece<R>* T = bessel_table<R>();
