@@ -468,6 +468,30 @@ def run_reference_gpu(args):
     print(json.dumps(line), flush=True)
 
 
+def run_ingest(args):
+    """Snapshot admission: the plain-path workload's dump read and made resident with the host decode (16 OpenMP
+    threads on the GPU box) and with the GPU decode (cells decoded on the device while the dump streams in).  The dump
+    is read once first so that both runs read it from the page cache.  Prints one JSON line."""
+    import phoenix_b200 as P
+    dump, grid = snapshot_files(WORKLOAD)
+    with open(dump, "rb") as f:
+        while f.read(64 << 20):
+            pass
+    out = {"workload": "ingest", "config": {"dump_bytes": os.path.getsize(dump),
+                                            "snapshot": "192x96x96 base grid, 8^3 blocks, 3 AMR levels (15.6M cells)"}}
+    for gpu in (False, True, False, True):
+        t0 = time.perf_counter()
+        s = P.Snapshot.load(dump, grid, nlevels=WORKLOAD["nlevels"], gpu_decode=gpu)
+        wall = time.perf_counter() - t0
+        i = s.info()
+        s.close()
+        out["gpu_decode" if gpu else "host_decode"] = {"wall_s": wall, "read_s": i["read_s"],
+                                                       "decode_s": i["decode_s"], "upload_s": i["upload_s"],
+                                                       "cells_per_s": i["nleafs"] * i["cells"] / wall}
+    out["host_threads"] = os.cpu_count()
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -479,7 +503,7 @@ def main():
     ap.add_argument("--period", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="plain", choices=["plain", "batch", "serve"],
+    ap.add_argument("--workload", default="plain", choices=["plain", "batch", "serve", "ingest"],
                     help="plain: the headline single-image path (default); batch: the 128-image sweep; "
                          "serve: Poisson request streams through the server")
     ap.add_argument("--requests", type=int, default=0, help="serve: requests per stream")
@@ -494,6 +518,8 @@ def main():
         return run_batch(args)
     if args.workload == "serve":
         return run_serve(args)
+    if args.workload == "ingest":
+        return run_ingest(args)
 
     import torch
     import torch.distributed as dist

@@ -43,7 +43,9 @@ enum {
 
 /* Snapshot creation flags. */
 enum {
-  PHX_SNAP_F64_PRIMS = 1 /* also keep FP64 primitives on the device (FP64 renders then read them) */
+  PHX_SNAP_F64_PRIMS = 1, /* also keep FP64 primitives on the device (FP64 renders then read them) */
+  PHX_SNAP_GPU_DECODE = 2 /* phx_snapshot_load: decode conserved -> primitive on the GPU while the dump streams in
+                             (the reference's grmhd.gpu_decode, src/device/kernel.cu:105-112, 200-260) */
 };
 
 /* One (pixel, frequency) result; binary-identical to the reference's core::pixel::FreqOut
@@ -137,6 +139,23 @@ void phx_bhac_free(PhxHostSnapshot* h);
 
 /* Device bytes held by a snapshot. */
 int64_t phx_snapshot_bytes(const PhxSnapshot* s);
+
+/* Shape, constants and load timings of a resident snapshot. */
+typedef struct {
+  int64_t nleafs;
+  int32_t cells, nlevels, nx[3], ng[3];
+  double a, hslope, gam, x_lo[3], x_hi[3];
+  int32_t has_f64_prims, gpu_decoded;
+  int64_t bytes;
+  double read_s;    /* reading the dump (with the host decode when not decoded on the GPU) */
+  double decode_s;  /* GPU decode: streaming the cells in, copies and decode kernels */
+  double upload_s;  /* device allocation and uploads of phx_snapshot_create */
+} PhxSnapshotInfo;
+int phx_snapshot_info(const PhxSnapshot* s, PhxSnapshotInfo* info);
+
+/* Copies the device primitives to host memory ([nleafs][cells][8]; either pointer may be NULL; prim_f64 needs a
+ * snapshot with FP64 primitives). */
+int phx_snapshot_download(const PhxSnapshot* s, float* prim_f32, double* prim_f64);
 
 /* Pixel job list i * img_height + j, Morton-ordered (host::jobs::schedule with morton = true,
  * src/host/render/jobs.hpp:18-45).  jobs holds img_width * img_height entries. */

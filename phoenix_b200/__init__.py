@@ -30,14 +30,29 @@ class Snapshot:
 
     @classmethod
     def load(cls, dump: str, grid: str, nspin: int = 3, bpol: int = 1, sfc: bool = True, nlevels: int = -1,
-             f64_prims: bool = False) -> "Snapshot":
-        """Read a BHAC dump + grid file (config.toml [grmhd] keys), decode it on the host and upload it."""
+             f64_prims: bool = False, gpu_decode: bool = False) -> "Snapshot":
+        """Read a BHAC dump + grid file (config.toml [grmhd] keys) and make it resident; the cells are decoded on the
+        host, or on the GPU while the dump streams in (gpu_decode)."""
         L = native.lib()
         opt = native.PhxReadOptions(nspin, bpol, 1 if sfc else 0, nlevels)
         h = C.c_void_p()
-        native.check(L.phx_snapshot_load(dump.encode(), grid.encode(), C.byref(opt),
-                                         native.SNAP_F64_PRIMS if f64_prims else 0, C.byref(h)))
+        flags = (native.SNAP_F64_PRIMS if f64_prims else 0) | (native.SNAP_GPU_DECODE if gpu_decode else 0)
+        native.check(L.phx_snapshot_load(dump.encode(), grid.encode(), C.byref(opt), flags, C.byref(h)))
         return cls(h.value)
+
+    def info(self) -> dict:
+        i = native.PhxSnapshotInfo()
+        native.check(native.lib().phx_snapshot_info(self._h, C.byref(i)))
+        return i.as_dict()
+
+    def download(self, f64: bool = False):
+        """The device primitives as numpy arrays [nleafs, cells, 8] (FP32, and FP64 when asked)."""
+        i = self.info()
+        shape = (i["nleafs"], i["cells"], 8)
+        pf = np.empty(shape, np.float32)
+        pd = np.empty(shape, np.float64) if f64 else None
+        native.check(native.lib().phx_snapshot_download(self._h, pf.ctypes.data, pd.ctypes.data if f64 else None))
+        return (pf, pd) if f64 else pf
 
     @classmethod
     def from_arrays(cls, *, nx, ng, nlevels, a, hslope, gam, x_lo, x_hi, lb, dxc, prim_f32, level_maps,

@@ -61,7 +61,7 @@ cudaError_t dispatch(PhxSnapshot* s, const PhxRenderParams& p, const int32_t* d_
   return cudaErrorInvalidValue;
 }
 
-void validate_desc(const PhxSnapshotDesc* d) {
+void validate_desc(const PhxSnapshotDesc* d, bool defer_prims = false) {
   auto bad = [](const std::string& m) { throw std::invalid_argument(m); };
   if (!d) bad("null snapshot descriptor");
   if (d->nleafs < 1) bad("nleafs must be >= 1");
@@ -70,7 +70,8 @@ void validate_desc(const PhxSnapshotDesc* d) {
     if (d->nx[k] < 1 || d->ng[k] < 1) bad("nx and ng must be positive");
     if (!(d->x_hi[k] > d->x_lo[k])) bad("empty domain");
   }
-  if (!d->lb || !d->dxc || !d->prim_f32 || !d->level_map) bad("lb, dxc, prim_f32 and level_map are required");
+  if (!d->lb || !d->dxc || (!d->prim_f32 && !defer_prims) || !d->level_map)
+    bad("lb, dxc, prim_f32 and level_map are required");
   if (!(std::fabs(d->a) < 1.0)) bad("spin must satisfy |a| < 1");
   const size_t top = (size_t)1 << (d->nlevels - 1);
   const size_t slots = d->ng[0] * top * d->ng[1] * top * d->ng[2] * top;
@@ -85,8 +86,10 @@ void validate_desc(const PhxSnapshotDesc* d) {
   }
 }
 
-PhxSnapshot* create_snapshot(const PhxSnapshotDesc* d, int32_t flags) {
-  validate_desc(d);
+// defer_prims: allocate the primitive pool without filling it (the GPU decode writes it).
+PhxSnapshot* create_snapshot(const PhxSnapshotDesc* d, int32_t flags, bool defer_prims = false) {
+  validate_desc(d, defer_prims);
+  const auto t0 = std::chrono::steady_clock::now();
   auto s = std::make_unique<PhxSnapshot>();
   ck(cudaGetDevice(&s->device), "cudaGetDevice");
   cudaDeviceProp prop;
@@ -123,12 +126,22 @@ PhxSnapshot* create_snapshot(const PhxSnapshotDesc* d, int32_t flags) {
   s->dxc_f = dev_upload(dxf.data(), n3, s->owned);
   s->lb_d = dev_upload(d->lb, n3, s->owned);
   s->dxc_d = dev_upload(d->dxc, n3, s->owned);
-  s->prim_f = dev_upload(d->prim_f32, nprim, s->owned);
-  if ((flags & PHX_SNAP_F64_PRIMS) && d->prim_f64) s->prim_d = dev_upload(d->prim_f64, nprim, s->owned);
+  if (defer_prims) {
+    ck(cudaMalloc((void**)&s->prim_f, nprim * sizeof(float)), "cudaMalloc primitives");
+    s->owned.push_back(s->prim_f);
+    if (flags & PHX_SNAP_F64_PRIMS) {
+      ck(cudaMalloc((void**)&s->prim_d, nprim * sizeof(double)), "cudaMalloc primitives");
+      s->owned.push_back(s->prim_d);
+    }
+  } else {
+    s->prim_f = dev_upload(d->prim_f32, nprim, s->owned);
+    if ((flags & PHX_SNAP_F64_PRIMS) && d->prim_f64) s->prim_d = dev_upload(d->prim_f64, nprim, s->owned);
+  }
   s->fmap = dev_upload(flat.data(), flat.size(), s->owned);
   s->bytes = (int64_t)(n3 * (2 * sizeof(float) + 2 * sizeof(double)) + nprim * sizeof(float) +
                        (s->prim_d ? nprim * sizeof(double) : 0) + flat.size() * sizeof(int32_t));
   ck(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  s->upload_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   return s.release();
 }
 
@@ -221,18 +234,83 @@ int phx_snapshot_load(const char* dump_file, const char* grid_file, const PhxRea
                       PhxSnapshot** out) {
   return guarded([&]() -> int {
     if (!out) throw std::invalid_argument("null output handle");
+    if (flags & PHX_SNAP_GPU_DECODE) {
+      if (!dump_file || !grid_file) throw std::invalid_argument("null argument");
+      phx::SnapshotOptions o;
+      if (opt) {
+        o.nspin = opt->nspin;
+        o.bpol = opt->bpol;
+        o.sfc = opt->sfc != 0;
+        o.nlevels = opt->nlevels;
+      }
+      const auto t0 = std::chrono::steady_clock::now();
+      PhxHostSnapshot meta;
+      meta.h = phx::load_bhac_meta(dump_file, grid_file, o);
+      for (int L = 0; L < meta.h.nlevels; L++) meta.maps.push_back(meta.h.level_map[L].data());
+      PhxSnapshotDesc d;
+      phx_bhac_describe(&meta, &d);
+      const double read_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      std::unique_ptr<PhxSnapshot> s(create_snapshot(&d, flags, true));
+      s->decode_s = gpu_decode(s.get(), dump_file, meta.h, o.bpol);
+      s->read_s = read_s;
+      s->gpu_decoded = true;
+      *out = s.release();
+      return PHX_OK;
+    }
+    const auto t0 = std::chrono::steady_clock::now();
     PhxHostSnapshot* hs = nullptr;
     const int rc = phx_bhac_read(dump_file, grid_file, opt, flags, &hs);
     if (rc != PHX_OK) return rc;
     std::unique_ptr<PhxHostSnapshot> guard(hs);
     PhxSnapshotDesc d;
     phx_bhac_describe(hs, &d);
+    const double read_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     *out = create_snapshot(&d, flags);
+    (*out)->read_s = read_s;
     return PHX_OK;
   });
 }
 
 void phx_snapshot_destroy(PhxSnapshot* s) { delete s; }
+
+int phx_snapshot_info(const PhxSnapshot* s, PhxSnapshotInfo* info) {
+  return guarded([&]() -> int {
+    if (!s || !info) throw std::invalid_argument("null argument");
+    std::memset(info, 0, sizeof *info);
+    info->nleafs = s->nleafs;
+    info->cells = s->cells;
+    info->nlevels = s->nlevels;
+    for (int k = 0; k < 3; k++) {
+      info->nx[k] = s->nx[k];
+      info->ng[k] = s->ng[k];
+      info->x_lo[k] = s->x_lo[k];
+      info->x_hi[k] = s->x_hi[k];
+    }
+    info->a = s->a;
+    info->hslope = s->hslope;
+    info->gam = s->gam;
+    info->has_f64_prims = s->prim_d != nullptr;
+    info->gpu_decoded = s->gpu_decoded;
+    info->bytes = s->bytes;
+    info->read_s = s->read_s;
+    info->decode_s = s->decode_s;
+    info->upload_s = s->upload_s;
+    return PHX_OK;
+  });
+}
+
+int phx_snapshot_download(const PhxSnapshot* s, float* prim_f32, double* prim_f64) {
+  return guarded([&]() -> int {
+    if (!s) throw std::invalid_argument("null snapshot");
+    const size_t nprim = (size_t)s->nleafs * s->cells * phx::kNPrim;
+    if (prim_f32) ck(cudaMemcpy(prim_f32, s->prim_f, nprim * sizeof(float), cudaMemcpyDeviceToHost), "D2H primitives");
+    if (prim_f64) {
+      if (!s->prim_d) throw std::invalid_argument("the snapshot keeps no FP64 primitives");
+      ck(cudaMemcpy(prim_f64, s->prim_d, nprim * sizeof(double), cudaMemcpyDeviceToHost), "D2H primitives");
+    }
+    return PHX_OK;
+  });
+}
 
 int64_t phx_snapshot_bytes(const PhxSnapshot* s) { return s ? s->bytes : 0; }
 

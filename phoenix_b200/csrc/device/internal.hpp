@@ -86,6 +86,8 @@ struct PhxSnapshot {
   int64_t bytes = 0;
   std::vector<void*> owned;
   phx_capi::Workspace ws;
+  double read_s = 0.0, decode_s = 0.0, upload_s = 0.0;  // load timings (read + host decode are in read_s)
+  bool gpu_decoded = false;
   cudaStream_t stream = nullptr;
   ~PhxSnapshot() {
     if (stream) cudaStreamDestroy(stream);
@@ -152,5 +154,8 @@ int guarded(F&& f) {
     return fail(PHX_E_IO, e.what());
   }
 }
+
+// GPU decode of a dump into s's allocated primitive pool (decode.cu); returns seconds.
+double gpu_decode(PhxSnapshot* s, const std::string& dump, const phx::HostSnapshot& meta, int bpol);
 
 }  // namespace phx_capi

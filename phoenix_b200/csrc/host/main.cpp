@@ -136,8 +136,8 @@ int main(int argc, char** argv) {
   okmsg("Load config file      \"%s\"", cfgpath.c_str());
   const double t_model = now_s();
   PhxSnapshot* snap = nullptr;
-  if (phx_snapshot_load(cfg.dump_file.c_str(), cfg.grid_file.c_str(), &cfg.read,
-                        p.precision == PHX_PREC_FP64 ? PHX_SNAP_F64_PRIMS : 0, &snap) != PHX_OK) {
+  const int32_t flags = (p.precision == PHX_PREC_FP64 ? PHX_SNAP_F64_PRIMS : 0) | (cfg.gpu_decode ? PHX_SNAP_GPU_DECODE : 0);
+  if (phx_snapshot_load(cfg.dump_file.c_str(), cfg.grid_file.c_str(), &cfg.read, flags, &snap) != PHX_OK) {
     failmsg("%s", phx_last_error());
     return EXIT_FAILURE;
   }

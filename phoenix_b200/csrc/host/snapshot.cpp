@@ -99,7 +99,7 @@ std::vector<int32_t> flatten_level_maps(const std::vector<std::vector<int32_t>>&
   return flat;
 }
 
-HostSnapshot load_bhac(const std::string& dump, const std::string& grid, const SnapshotOptions& opt) {
+HostSnapshot load_bhac_meta(const std::string& dump, const std::string& grid, const SnapshotOptions& opt) {
   HostSnapshot s;
   double xmin[3], xmax[3];
   read_grid_file(grid, s.nxlone, xmin, xmax, &s.hslope);
@@ -193,6 +193,32 @@ HostSnapshot load_bhac(const std::string& dump, const std::string& grid, const S
     }
   }
 
+  return s;
+}
+
+void stream_leaf_blocks(const std::string& dump, const HostSnapshot& s, int chunk,
+                        const std::function<double*(int, int)>& next_buffer,
+                        const std::function<void(int, int, const double*)>& ready) {
+  FilePtr fp(std::fopen(dump.c_str(), "rb"));
+  FILE* f = fp.get();
+  if (!f) throw std::runtime_error("Can't open " + dump);
+  const size_t leaf_doubles = (size_t)s.nwini * s.cells;
+  const long long stag_bytes = (long long)(s.nx[0] + 1) * (s.nx[1] + 1) * (s.nx[2] + 1) * s.nws * 8;
+  for (int l0 = 0; l0 < s.nleafs; l0 += chunk) {
+    const int nl = std::min(chunk, s.nleafs - l0);
+    double* buf = next_buffer(l0, nl);
+    for (int q = 0; q < nl; q++) {
+      if (std::fread(buf + (size_t)q * leaf_doubles, sizeof(double), leaf_doubles, f) != leaf_doubles)
+        throw std::runtime_error("short read in the data, leaf " + std::to_string(l0 + q));
+      if (stag_bytes && std::fseek(f, (long)stag_bytes, SEEK_CUR) != 0)
+        throw std::runtime_error("short read in the data, leaf " + std::to_string(l0 + q));
+    }
+    ready(l0, nl, buf);
+  }
+}
+
+HostSnapshot load_bhac(const std::string& dump, const std::string& grid, const SnapshotOptions& opt) {
+  HostSnapshot s = load_bhac_meta(dump, grid, opt);
   // decode: stream the leaf blocks, conserved -> primitive per cell in parallel
   const size_t leaf_doubles = (size_t)s.nwini * s.cells;
   const size_t nprim = (size_t)s.nleafs * s.cells * kNPrim;
@@ -200,29 +226,23 @@ HostSnapshot load_bhac(const std::string& dump, const std::string& grid, const S
   if (opt.keep_f64) s.prim_f64.assign(nprim, 0.0);
   const int chunk = 256;
   std::vector<double> raw((size_t)chunk * leaf_doubles);
-  if (std::fseek(f, 0, SEEK_SET) != 0) throw std::runtime_error("seek failed on " + dump);
-  for (int l0 = 0; l0 < s.nleafs; l0 += chunk) {
-    const int nl = std::min(chunk, s.nleafs - l0);
-    for (int q = 0; q < nl; q++) {
-      if (std::fread(raw.data() + (size_t)q * leaf_doubles, sizeof(double), leaf_doubles, f) != leaf_doubles)
-        throw std::runtime_error("short read in the data, leaf " + std::to_string(l0 + q));
-      if (stag_bytes && std::fseek(f, (long)stag_bytes, SEEK_CUR) != 0)
-        throw std::runtime_error("short read in the data, leaf " + std::to_string(l0 + q));
-    }
+  stream_leaf_blocks(
+      dump, s, chunk, [&](int, int) { return raw.data(); },
+      [&](int l0, int nl, const double* buf) {
 #pragma omp parallel for schedule(dynamic, 1)
-    for (int q = 0; q < nl; q++) {
-      const size_t l = (size_t)l0 + q;
-      for (int cell = 0; cell < s.cells; cell++) {
-        double p[kNPrim];
-        cons_to_prim(s.a, s.hslope, s.gam, opt.bpol, s.nwini, s.nx, &s.lb[3 * l], &s.dxc[3 * l],
-                     raw.data() + (size_t)q * leaf_doubles, cell, p);
-        const size_t o = (l * s.cells + cell) * kNPrim;
-        for (int v = 0; v < kNPrim; v++) s.prim_f32[o + v] = (float)p[v];
-        if (opt.keep_f64)
-          for (int v = 0; v < kNPrim; v++) s.prim_f64[o + v] = p[v];
-      }
-    }
-  }
+        for (int q = 0; q < nl; q++) {
+          const size_t l = (size_t)l0 + q;
+          for (int cell = 0; cell < s.cells; cell++) {
+            double p[kNPrim];
+            cons_to_prim(s.a, s.hslope, s.gam, opt.bpol, s.nwini, s.nx, &s.lb[3 * l], &s.dxc[3 * l],
+                         buf + (size_t)q * leaf_doubles, cell, p);
+            const size_t o = (l * s.cells + cell) * kNPrim;
+            for (int v = 0; v < kNPrim; v++) s.prim_f32[o + v] = (float)p[v];
+            if (opt.keep_f64)
+              for (int v = 0; v < kNPrim; v++) s.prim_f64[o + v] = p[v];
+          }
+        }
+      });
   return s;
 }
 

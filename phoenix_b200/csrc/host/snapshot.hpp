@@ -6,6 +6,7 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -34,6 +35,16 @@ struct HostSnapshot {
 // Throws std::runtime_error with the reference's messages on malformed input.
 void read_grid_file(const std::string& path, int nxlone[3], double xprobmin[3], double xprobmax[3], double* hslope);
 HostSnapshot load_bhac(const std::string& dump, const std::string& grid, const SnapshotOptions& opt);
+
+// The reader without the cell data: header, forest, leaf geometry and level maps (prim_* left empty).
+HostSnapshot load_bhac_meta(const std::string& dump, const std::string& grid, const SnapshotOptions& opt);
+
+// Streams the leaves' conserved blocks (nwini arrays of `cells` doubles per leaf, staggered fields skipped) in chunks
+// of at most `chunk` leaves.  next_buffer(l0, nl) returns where chunk [l0, l0 + nl) is read to (room for nl blocks);
+// ready(l0, nl, buf) is called once it holds them.
+void stream_leaf_blocks(const std::string& dump, const HostSnapshot& s, int chunk,
+                        const std::function<double*(int, int)>& next_buffer,
+                        const std::function<void(int, int, const double*)>& ready);
 
 // Finest-level leaf map: slot (i,j,k) of level nlevels-1 holds the first leaf found walking the per-level maps from
 // the coarsest level (what the reference's find_leaf_map returns for any point in that slot).

@@ -19,6 +19,7 @@ PHX_OK, PHX_E_INVALID, PHX_E_IO, PHX_E_CUDA, PHX_E_TIMEOUT, PHX_E_UNSUPPORTED = 
 PREC_FP32, PREC_FP64, PREC_MIXED = 0, 1, 2
 PRECISIONS = {"fp32": PREC_FP32, "fp64": PREC_FP64, "mixed": PREC_MIXED}
 SNAP_F64_PRIMS = 1
+SNAP_GPU_DECODE = 2
 NOALLOC_MAX_JOBS = 1 << 20
 NUM_COUNTERS = 16
 CTR = dict(queue=0, steps=1, nplasma=2, bad=3, scans=4, fp64_steps=5, fp64_ops=6, rays=7)
@@ -29,7 +30,8 @@ EXPORTS = ["phx_default_params", "phx_snapshot_create", "phx_snapshot_load", "ph
            "phx_version", "phx_default_batch_options", "phx_batch_create", "phx_batch_launch", "phx_batch_run",
            "phx_batch_result", "phx_batch_device_result", "phx_batch_tuning", "phx_batch_destroy",
            "phx_default_server_options", "phx_server_create", "phx_server_submit", "phx_server_poll",
-           "phx_server_wait", "phx_server_result", "phx_server_stats", "phx_server_destroy"]
+           "phx_server_wait", "phx_server_result", "phx_server_stats", "phx_server_destroy",
+           "phx_snapshot_info", "phx_snapshot_download"]
 REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
 TUNE_MAX_CANDIDATES = 16
 
@@ -104,6 +106,21 @@ class PhxBatchTuning(C.Structure):
         d = {name: getattr(self, name) for name, _ in self._fields_ if not name.startswith("cand_")}
         d["candidates"] = [dict(blocks_per_sm=self.cand_blocks_per_sm[i], period=self.cand_period[i],
                                 ms=self.cand_ms[i]) for i in range(n)]
+        return d
+
+
+class PhxSnapshotInfo(C.Structure):
+    _fields_ = [("nleafs", C.c_int64), ("cells", C.c_int32), ("nlevels", C.c_int32), ("nx", C.c_int32 * 3),
+                ("ng", C.c_int32 * 3), ("a", C.c_double), ("hslope", C.c_double), ("gam", C.c_double),
+                ("x_lo", C.c_double * 3), ("x_hi", C.c_double * 3), ("has_f64_prims", C.c_int32),
+                ("gpu_decoded", C.c_int32), ("bytes", C.c_int64), ("read_s", C.c_double), ("decode_s", C.c_double),
+                ("upload_s", C.c_double)]
+
+    def as_dict(self):
+        d = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            d[name] = list(v) if hasattr(v, "__len__") else v
         return d
 
 
@@ -182,6 +199,10 @@ def lib():
     L.phx_batch_tuning.argtypes = [C.c_void_p, P(PhxBatchTuning)]
     L.phx_batch_destroy.argtypes = [C.c_void_p]
     L.phx_batch_destroy.restype = None
+    L.phx_snapshot_info.argtypes = [C.c_void_p, P(PhxSnapshotInfo)]
+    L.phx_snapshot_info.restype = C.c_int
+    L.phx_snapshot_download.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    L.phx_snapshot_download.restype = C.c_int
     L.phx_default_server_options.argtypes = [P(PhxServerOptions)]
     L.phx_default_server_options.restype = None
     L.phx_server_create.argtypes = [C.c_void_p, C.c_int32, P(PhxServerOptions), P(C.c_void_p)]

@@ -17,8 +17,8 @@ pytestmark = pytest.mark.gpu
 FLUX = re.compile(r"Flux at (\S+) Hz \(Jy\): \S*I\S* (\S+) \S*Q\S* (\S+) \S*U\S* (\S+) \S*V\S* (\S+)")
 
 
-@pytest.mark.parametrize("precision", ["fp32", "fp64"])
-def test_cli_end_to_end(built, snapshots, oracle_results, tmp_path, precision):
+@pytest.mark.parametrize("precision,gpu_decode", [("fp32", False), ("fp64", False), ("fp32", True)])
+def test_cli_end_to_end(built, snapshots, oracle_results, tmp_path, precision, gpu_decode):
     name = "thick"
     case = CASES[name]
     dump, grid, _ = snapshots[case["snapshot"]]
@@ -26,7 +26,8 @@ def test_cli_end_to_end(built, snapshots, oracle_results, tmp_path, precision):
     cfg = tmp_path / "config.toml"
     write_config(str(cfg), case, dump, grid, str(out))
     env = dict(os.environ, PHX_PRECISION=precision)
-    r = subprocess.run([built["cli"], str(cfg), "output.image=both", "output.block_size=8"], capture_output=True,
+    r = subprocess.run([built["cli"], str(cfg), "output.image=both", "output.block_size=8",
+                        "grmhd.gpu_decode=" + ("true" if gpu_decode else "false")], capture_output=True,
                        text=True, env=env, timeout=600)
     assert r.returncode == 0, r.stderr
     lines = FLUX.findall(re.sub(r"\x1b\[[0-9;]*m", "", r.stderr))
@@ -50,7 +51,7 @@ def test_cli_end_to_end(built, snapshots, oracle_results, tmp_path, precision):
     # the file holds exactly what the library renders for the same parameters
     import phoenix_b200 as P
     from tests.golden.cases import case_params
-    with P.Snapshot.load(dump, grid, nlevels=3, f64_prims=precision == "fp64") as snap:
+    with P.Snapshot.load(dump, grid, nlevels=3, f64_prims=precision == "fp64", gpu_decode=gpu_decode) as snap:
         mine, _ = snap.render(P.make_params(precision=precision, **case_params(name)))
     np.testing.assert_array_equal(img, mine[ii, jj, 0, 0] * 1e23)
     assert (out / "image_0.dat").exists() and (out / "image_2.dat").exists() and (out / "spectrum.dat").exists()

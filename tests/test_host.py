@@ -131,7 +131,7 @@ def test_ctypes_structs_match_the_header(tmp_path):
                "PhxFreqOut": native.PhxFreqOut, "PhxBatchItem": native.PhxBatchItem,
                "PhxBatchOptions": native.PhxBatchOptions, "PhxBatchTuning": native.PhxBatchTuning,
                "PhxServerOptions": native.PhxServerOptions, "PhxRequestTiming": native.PhxRequestTiming,
-               "PhxServerStats": native.PhxServerStats}
+               "PhxServerStats": native.PhxServerStats, "PhxSnapshotInfo": native.PhxSnapshotInfo}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "phoenix_b200.h"', "int main(void) {"]
     for name, cls in structs.items():
         lines.append(f'  printf("{name} size %zu\\n", sizeof({name}));')
