@@ -41,10 +41,10 @@ FLOPS = dict(step=1800.0, sample=900.0, freq=850.0)
 # of the trilinear gather (256 B); per step the flattened leaf-map entry (4 B) and the leaf's lb/dxc (24 B); per ray
 # its job index (4 B) and one 48 B FreqOut record per frequency.
 BYTES = dict(sample=256.0, step=28.0, ray=4.0, ray_freq=48.0)
-# DRAM bytes (read + write) per ray-step of k_march, from the ncu capture of the same snapshot at 256^2 pixels
-# (profiles/k_march_plain_gpu_256.md): dram__bytes_read.sum + dram__bytes_write.sum = 572.5 MB over the launch's
-# ~197M ray-steps.  Scaled to a full launch by its ray-steps.
-DRAM_BYTES_PER_STEP = 2.90
+# DRAM bytes (read + write) per ray-step of k_march, from the ncu capture of one launch of this workload
+# (profiles/k_march_plain_gpu_512.md): dram__bytes_read.sum + dram__bytes_write.sum = 805.2 MB over the launch's
+# 726.6M ray-steps.  Scaled to the average launch by its ray-steps.
+DRAM_BYTES_PER_STEP = 1.108
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 
 
