@@ -424,6 +424,19 @@ def run_serve(args):
     print(json.dumps(line), flush=True)
 
 
+def max_time_sum_work(t_local, work_local, device, world):
+    """Whole-job figures of N independent replicas: the slowest rank's time and the work of all ranks (every rank
+    takes part in the same two collectives)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(t_local)], dtype=torch.float64, device=device)
+    n = torch.tensor([float(work_local)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(n, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(n.item())
+
+
 def run_reference_gpu(args):
     """The reference's own CUDA kernel (src/device/kernel.cu built for sm_100a from its sources, FP32, one frequency
     slot, 128 threads x 3 blocks/SM as its CMake defaults) on the plain-path workload, timed by its own CUDA events
@@ -593,13 +606,8 @@ def main():
     clocks = clk.summary()
     ms = sum(a.elapsed_time(b) for a, b in ev)
     kms = [a.elapsed_time(b) for row in kev for a, b in row]
-    t_local = torch.tensor([ms], dtype=torch.float64, device=dev)
-    n_local = torch.tensor([steps_total], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t_local, op=dist.ReduceOp.MAX)
-        dist.all_reduce(n_local, op=dist.ReduceOp.SUM)
-    ms_max = float(t_local.item())
-    value = float(n_local.item()) / (ms_max * 1e-3)
+    ms_max, steps_all = max_time_sum_work(ms, steps_total, dev, world)
+    value = steps_all / (ms_max * 1e-3)
 
     # end to end through the public API: pinned host job list in, host FreqOut image out, every step
     e2e = None
@@ -618,12 +626,8 @@ def main():
                 _, info = snap.render(p, jobs=jobs_h.numpy(), out=outs[k].numpy())
                 e_steps += info["steps"]
         e_s = time.perf_counter() - t1
-        te = torch.tensor([e_s], dtype=torch.float64, device=dev)
-        ne = torch.tensor([e_steps], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-            dist.all_reduce(ne, op=dist.ReduceOp.SUM)
-        e2e = {"value": float(ne.item()) / float(te.item()), "unit": "ray-steps/s",
+        te_max, ne_all = max_time_sum_work(e_s, e_steps, dev, world)
+        e2e = {"value": ne_all / te_max, "unit": "ray-steps/s",
                "h2d_bytes_per_step": len(params) * npix * 4,
                "d2h_bytes_per_step": len(params) * (npix * 48 + P.NUM_COUNTERS * 8)}
 
