@@ -100,22 +100,16 @@ PHX_HD void camera_photon(const CameraSpec& cs, double alpha, double beta, doubl
 //   perp^mu = -eps^{mu nu rho sigma} U_nu k_rho b_sigma / (sqrt(-g) omega N)   (RAPTOR's observer tetrad, the
 // reference's create_observer_tetrad, core/geometry/tetrad.hpp:51-101).  omega = -k.U is returned too.
 template <class R>
-PHX_HD void observer_axes(const Cov<R>& g, R sqrtg, const R k[4], const R U[4], const R b[4], R perp[4], R para[4],
-                          R* omega_out) {
-  const R omega = -dot(g, k, U);
+PHX_HD void observer_axes_lowered(R sqrtg, const R k[4], const R U[4], const R b[4], const R kd[4], const R Ud[4],
+                                  const R bd[4], R omega, R kb, R Ub, R bb, R perp[4], R para[4]) {
   const R iomega = R(1) / omega;
   R eK[4];
   for (int i = 0; i < 4; i++) eK[i] = k[i] * iomega - U[i];
-  const R Beta = dot(g, U, b);
-  const R Cc = dot(g, k, b) * iomega - Beta;
-  const R b2 = dot(g, b, b);
-  const R Nc = sqrt_t(b2 + Beta * Beta - Cc * Cc);
+  const R Beta = Ub;
+  const R Cc = kb * iomega - Beta;
+  const R Nc = sqrt_t(bb + Beta * Beta - Cc * Cc);
   const R iNc = R(1) / Nc;
   for (int i = 0; i < 4; i++) para[i] = (b[i] + Beta * U[i] - Cc * eK[i]) * iNc;
-  R Ud[4], kd[4], bd[4];
-  symv(g, U, Ud);
-  symv(g, k, kd);
-  symv(g, b, bd);
   const R s = -iomega * iNc / sqrtg;
   // generalized cross product: perp^i = (-1)^i det[U, k, b] over the three columns other than i
   const R m01 = kd[0] * bd[1] - kd[1] * bd[0], m02 = kd[0] * bd[2] - kd[2] * bd[0], m03 = kd[0] * bd[3] - kd[3] * bd[0];
@@ -124,6 +118,17 @@ PHX_HD void observer_axes(const Cov<R>& g, R sqrtg, const R k[4], const R U[4], 
   perp[1] = -s * (Ud[0] * m23 - Ud[2] * m03 + Ud[3] * m02);
   perp[2] = s * (Ud[0] * m13 - Ud[1] * m03 + Ud[3] * m01);
   perp[3] = -s * (Ud[0] * m12 - Ud[1] * m02 + Ud[2] * m01);
+}
+
+template <class R>
+PHX_HD void observer_axes(const Cov<R>& g, R sqrtg, const R k[4], const R U[4], const R b[4], R perp[4], R para[4],
+                          R* omega_out) {
+  R Ud[4], kd[4], bd[4];
+  symv(g, U, Ud);
+  symv(g, k, kd);
+  symv(g, b, bd);
+  const R omega = -dot4(kd, U);
+  observer_axes_lowered(sqrtg, k, U, b, kd, Ud, bd, omega, dot4(kd, b), dot4(Ud, b), dot4(bd, b), perp, para);
   *omega_out = omega;
 }
 

@@ -41,10 +41,11 @@ struct Contra {
   T tt, t1, x11, x13, x22, x33;
 };
 
+// Geometry at (r, x2) when r = exp(x1) is already known.
 template <class T>
-PHX_HD KerrPt<T> kerr_point(T a, T hs, T x1, T x2) {
+PHX_HD KerrPt<T> kerr_point_r(T a, T hs, T r, T x2) {
   KerrPt<T> p;
-  p.r = exp_t(x1);
+  p.r = r;
   // sin 2x2, cos 2x2 from one sincos of x2 (double-angle identities)
   T sx, cx;
   sincos_t(x2, &sx, &cx);
@@ -58,6 +59,11 @@ PHX_HD KerrPt<T> kerr_point(T a, T hs, T x1, T x2) {
   p.isig = T(1) / p.sig;
   p.q = T(2) * p.r * p.isig;
   return p;
+}
+
+template <class T>
+PHX_HD KerrPt<T> kerr_point(T a, T hs, T x1, T x2) {
+  return kerr_point_r(a, hs, exp_t(x1), x2);
 }
 
 template <class T>
@@ -88,6 +94,12 @@ PHX_HD Contra<T> contra_metric(const KerrPt<T>& p, T a) {
   u.x22 = iprod * p.s2;
   u.x33 = iprod * tp2;
   return u;
+}
+
+// Inner product of a lowered vector with a vector.
+template <class T>
+PHX_HD T dot4(const T Ud[4], const T V[4]) {
+  return Ud[0] * V[0] + Ud[1] * V[1] + Ud[2] * V[2] + Ud[3] * V[3];
 }
 
 // g_{mu nu} U^mu V^nu

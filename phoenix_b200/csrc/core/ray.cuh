@@ -101,6 +101,7 @@ struct Ray {
   bool pvalid, terminate;
   int steps, turns, bsign, nplasma, bad;
   R thdot_prev, dl_prev;
+  R pr;         // radius of the pending sample (exp of px[1], from the step that made it)
   int32_t pix;
   int leaf;     // leaf of the last step-size lookup (-1: none), tested before the leaf map
   R idxc[3];    // its inverse cell sizes
@@ -117,6 +118,7 @@ struct Ray {
     steps = turns = nplasma = bad = 0;
     bsign = st.bsign;
     thdot_prev = dl_prev = R(0);
+    pr = R(0);
     leaf = -1;
     idxc[0] = idxc[1] = idxc[2] = R(0);
   }
@@ -135,7 +137,7 @@ struct Ray {
     // The pending sample's plasma stage only runs inside rt_outer (the reference samples the fluid further out too,
     // but always discards it there: derive_fluid and process_sample both require r < rt_outer, and the sampler cache
     // the lookup seeds is local to that sample), so its cache seed is only needed then.
-    const bool pend_plasma = pvalid && exp_t(px[1]) < rc.rt_outer;
+    const bool pend_plasma = pvalid && pr < rc.rt_outer;
     const bool need_leaf = pend_plasma && alive;
     const bool need_dxc = alive && r < rc.rt_outer;
     int L = -1, right = -1;
@@ -157,7 +159,7 @@ struct Ray {
         }
         leaf = L;
       }
-      if (need_leaf) right = (exp_t(xw[1]) < R(1) || outside_domain(s, xw)) ? -1 : L;
+      if (need_leaf) right = (r < R(1) || outside_domain(s, xw)) ? -1 : L;  // wrapping keeps x1: exp(xw[1]) = r
     }
     if (pend_plasma) process_sample(s, rc, right, ctr);
 #pragma unroll
@@ -167,6 +169,7 @@ struct Ray {
       pF[i] = cF[i];
       if constexpr (kMixed) pxd[i] = (double)geo.hi[i] + (double)geo.lo[i];
     }
+    pr = r;
     pdl = dl_prev;
     pvalid = steps >= 1;
     if (!alive) return false;
@@ -207,9 +210,9 @@ struct Ray {
   // The plasma stage of the pending sample (the reference's process_sample, core/render/pixel.hpp:52-123).
   PHX_HD void process_sample(const SnapView<R, PT>& s, const RenderConsts<R>& rc, int right, RayCounters& ctr) {
     R k[4] = {pk[0], pk[1], pk[2], pk[3]};
-    const R r = exp_t(px[1]);
+    const R r = pr;
     {
-      const KerrPt<R> p0 = kerr_point(s.a, s.hs, px[1], px[2]);
+      const KerrPt<R> p0 = kerr_point_r(s.a, s.hs, r, px[2]);
       const Cov<R> g0 = cov_metric(p0, s.a);
       if (fabs_t(dot(g0, k, k)) > R(1e-6) && r > R(2)) {
         if constexpr (kMixed) {
@@ -250,7 +253,7 @@ struct Ray {
       for (int i = 0; i < 4; i++) x[i] = R(xd[i]);
     } else {
       wrap_coords(x);
-      if (exp_t(x[1]) < R(1)) return;
+      if (r < R(1)) return;  // exp(x[1]): wrapping keeps x1
       if (outside_domain(s, x)) return;
       if (ig == -1 || !inside_cached(s, ig, x)) {
         wrap_coords(x);
@@ -261,28 +264,36 @@ struct Ray {
       if (ig == -1) return;
       interp_prims<R, PT, !kComp>(s, ig, x, q);
     }
-    const KerrPt<R> p = kerr_point(s.a, s.hs, x[1], x[2]);
+    // (FP32 paths: x1 is the sample's own, so exp(x[1]) = r; the mixed path moved x to the FP64 placement)
+    const R rx = kMixed ? exp_t(x[1]) : r;
+    const KerrPt<R> p = kerr_point_r(s.a, s.hs, rx, x[2]);
     const Cov<R> g = cov_metric(p, s.a);
     const Contra<R> u = contra_metric(p, s.a);
     Fluid<R> fl;
-    if (!derive_fluid(rc.pv, s.gam, exp_t(x[1]), g, u, q, &fl)) return;
+    if (!derive_fluid(rc.pv, s.gam, rx, g, u, q, &fl)) return;
     if (!(r < rc.rt_outer)) return;
+    // k, U and B lowered once: every invariant below is then a 4-term inner product
+    R kd[4], Ud[4], Bd[4];
+    symv(g, k, kd);
+    symv(g, fl.U, Ud);
+    symv(g, fl.B, Bd);
+    const R kU = dot4(kd, fl.U), kB = dot4(kd, fl.B), UB = dot4(Ud, fl.B), BB = dot4(Bd, fl.B);
     // pitch angle of k to B in the plasma frame (tetrad.hpp:138-154): only its sine and cosine enter the
     // coefficients, so they are formed from mu = cos(pitch) directly; acos(mu) is 0 or pi exactly when mu = +-1
-    const R Bn = sqrt_t(fabs_t(dot(g, fl.B, fl.B)));
-    const R kU = dot(g, k, fl.U);
+    const R Bn = sqrt_t(fabs_t(BB));
     R sth = R(1), cth = R(0);
     if (Bn != R(0)) {
-      R mu = dot(g, k, fl.B) / (fabs_t(kU) * Bn);
+      R mu = kB / (fabs_t(kU) * Bn);
       if (fabs_t(mu) > R(1)) mu /= fabs_t(mu);
       if (mu == R(1) || mu == R(-1)) return;
       sth = sqrt_t((R(1) - mu) * (R(1) + mu));
       cth = mu;
     }
     // polarization axes of the plasma frame with B as reference direction; EVPA rotation from the transported F1
-    R perp[4], para[4], omega;
-    observer_axes(g, sqrt_neg_g(p), k, fl.U, fl.B, perp, para, &omega);
-    const R C = dot(g, perp, pF), S = dot(g, para, pF);
+    R perp[4], para[4], pFd[4];
+    observer_axes_lowered(sqrt_neg_g(p), k, fl.U, fl.B, kd, Ud, Bd, -kU, kB, UB, BB, perp, para);
+    symv(g, pF, pFd);
+    const R C = dot4(pFd, perp), S = dot4(pFd, para);
     const R inn = R(1) / (C * C + S * S);
     const R c2 = (C * C - S * S) * inn, s2 = R(2) * C * S * inn;
     const R ratio = -kU;  // nu_plasma / nu_camera
