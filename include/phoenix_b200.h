@@ -255,7 +255,8 @@ void phx_batch_destroy(PhxBatch* b);
  * memory_budget), and merges each admitted request's rays into one running queue kernel while earlier requests are
  * still on the GPU.  Each request's result equals what phx_render returns for it, to the rounding of the separately
  * compiled kernel, whatever else runs beside it.  The API is thread-safe; all CUDA work runs on the server's own
- * scheduler thread. */
+ * scheduler thread.  Large requests' tiles enter the queue a chunk at a time as it drains, and small requests enter
+ * whole ahead of them, so a small request that arrives behind a large one does not wait for all of the large one. */
 typedef struct PhxServer PhxServer;
 
 enum { PHX_REQ_QUEUED = 0, PHX_REQ_RUNNING = 1, PHX_REQ_DONE = 2, PHX_REQ_FAILED = 3 };
@@ -274,6 +275,10 @@ typedef struct {
   int64_t idle_limit;     /* polls after which an idle warp stops waiting and the kernel leaves, default 5e6 */
   double linger_ms;       /* idle time after which the scheduler stops the kernel, default 20 */
   int32_t poll_us;        /* scheduler polling interval, default 50 */
+  int32_t publish_chunk;  /* tiles a large request publishes at a time, default 64 */
+  int64_t backlog_rays;   /* published but unclaimed rays kept in the queue, 0 = two grid-loads of lanes */
+  int64_t small_rays;     /* requests of at most this many rays enter the queue whole, ahead of the large ones'
+                             remaining tiles (default 65536, a 256^2 image) */
 } PhxServerOptions;
 
 typedef struct {

@@ -94,6 +94,7 @@ struct Request {
   int32_t slot = -1;
   size_t out_off = 0, out_bytes = 0;
   int64_t rays = 0;
+  int64_t ntiles = 0, next_tile = 0;  // tiles of the request, and the first one not yet published
   std::vector<PhxFreqOut> host;
   PhxRequestTiming t{};
   Clock::time_point submitted;
@@ -130,6 +131,9 @@ struct PhxServer {
   bool kernel_running = false;
   int32_t next_slot = 0;
   unsigned long long tiles_published = 0;
+  unsigned long long tiles_reserved = 0;  // published + not yet published tiles of the admitted requests
+  std::vector<int64_t> unpublished;       // admitted requests with tiles left to publish, in admission order
+  unsigned long long* head_host = nullptr;  // pinned: the queue head read back each tick
   Clock::time_point idle_since;
   int64_t generations = 0;
   phx::LaunchShape lshape{};
@@ -155,6 +159,8 @@ struct PhxServer {
   void stop_kernel();
   void reap();
   void fail_inflight(const std::string& why);
+  void publish();
+  void reset_queue();
 };
 
 namespace {
@@ -214,6 +220,7 @@ PhxServer::~PhxServer() {
   cudaFree(ctl);
   cudaFree(counters);
   if (done_host) cudaFreeHost(done_host);
+  if (head_host) cudaFreeHost(head_host);
   if (staging) cudaFreeHost(staging);
 }
 
@@ -224,8 +231,7 @@ void PhxServer::start_generation() {
      "reset item counters");
   ck(cudaStreamSynchronize(control), "reset queue");
   std::memset(done_host, 0, sizeof(int32_t) * o.max_items);
-  next_slot = 0;
-  tiles_published = 0;
+  reset_queue();
   std::fill(slot_req.begin(), slot_req.end(), 0);
 }
 
@@ -246,7 +252,7 @@ void PhxServer::stop_kernel() {
 bool PhxServer::admit_one(Request& r) {
   const int64_t npix = (int64_t)r.p.img_width * r.p.img_height;
   const int64_t ntiles = (npix + o.tile_rays - 1) / o.tile_rays;
-  if (next_slot >= o.max_items || (long long)(tiles_published + ntiles) > o.max_tiles) return false;
+  if (next_slot >= o.max_items || (long long)(tiles_reserved + ntiles) > o.max_tiles) return false;
   const auto key = std::make_pair(r.p.img_width, r.p.img_height);
   size_t jobs_off = 0;
   auto jt = job_tables.find(key);
@@ -264,26 +270,20 @@ bool PhxServer::admit_one(Request& r) {
   }
   r.out_bytes = (size_t)npix * r.p.nfreqs * sizeof(PhxFreqOut);
   if (!alloc->alloc(r.out_bytes, &r.out_off)) return false;
-  if (!kernel_running && next_slot == 0 && tiles_published == 0) start_generation();
+  if (!kernel_running && next_slot == 0 && tiles_reserved == 0) start_generation();
   r.slot = next_slot++;
   r.rays = npix;
+  r.ntiles = ntiles;
+  r.next_tile = 0;
+  tiles_reserved += ntiles;
   slot_req[r.slot] = r.id;
-  // descriptor, tiles, tail: in this order on the control stream
-  unsigned char* st = staging;
-  write_item(r, reinterpret_cast<const int32_t*>(arena + jobs_off), st);
-  ck(cudaMemcpyAsync(static_cast<unsigned char*>(items) + item_bytes * r.slot, st, item_bytes, cudaMemcpyHostToDevice,
-                     control),
+  // the descriptor goes in now; its tiles are published by publish() as the queue drains
+  write_item(r, reinterpret_cast<const int32_t*>(arena + jobs_off), staging);
+  ck(cudaMemcpyAsync(static_cast<unsigned char*>(items) + item_bytes * r.slot, staging, item_bytes,
+                     cudaMemcpyHostToDevice, control),
      "H2D item");
-  phx::TileDesc* td = reinterpret_cast<phx::TileDesc*>(staging + ((item_bytes + 255) & ~(size_t)255));
-  for (int64_t t = 0; t < ntiles; t++)
-    td[t] = {r.slot, (int32_t)(t * o.tile_rays), (int32_t)std::min<int64_t>(o.tile_rays, npix - t * o.tile_rays), 0};
-  ck(cudaMemcpyAsync(tiles + tiles_published, td, ntiles * sizeof(phx::TileDesc), cudaMemcpyHostToDevice, control),
-     "H2D tiles");
-  tiles_published += ntiles;
-  unsigned long long* tail = reinterpret_cast<unsigned long long*>(staging + staging_bytes - 256);
-  *tail = tiles_published;
-  ck(cudaMemcpyAsync(ctl + phx::kQTail, tail, sizeof *tail, cudaMemcpyHostToDevice, control), "H2D tail");
-  ck(cudaStreamSynchronize(control), "publish");
+  ck(cudaStreamSynchronize(control), "H2D item");
+  unpublished.push_back(r.id);
   {
     std::lock_guard<std::mutex> lk(mu);
     r.state = PHX_REQ_RUNNING;
@@ -297,6 +297,63 @@ bool PhxServer::admit_one(Request& r) {
     generations++;
   }
   return true;
+}
+
+// Publishes tiles of the admitted requests.  Small requests (at most small_rays rays) go in whole as soon as they are
+// admitted; large ones go in first in, first out, a chunk at a time while the queue's backlog of published but
+// unclaimed rays is below about two grid-loads of lanes.  A small request that arrives behind a large one therefore
+// waits for that backlog, not for every ray of the large one, while the large ones keep their order and their rays'
+// coherence (interleaving them all round robin mixes snapshots and images in the caches and costs throughput).
+void PhxServer::publish() {
+  if (unpublished.empty()) return;
+  ck(cudaMemcpyAsync(head_host, ctl + phx::kQHead, sizeof *head_host, cudaMemcpyDeviceToHost, copy), "D2H head");
+  ck(cudaStreamSynchronize(copy), "D2H head");
+  const long long slots = (long long)tiles_published * o.tile_rays;
+  long long backlog = slots - (long long)*head_host;  // idle lanes' claims can pass the tail: then nothing is left
+  if (backlog < 0) backlog = 0;
+  const long long lanes = (long long)std::max(lshape.grid, 1) * std::max(lshape.block, 128);
+  const long long limit = o.backlog_rays > 0 ? o.backlog_rays : 2 * lanes;
+  phx::TileDesc* td = reinterpret_cast<phx::TileDesc*>(staging + ((item_bytes + 255) & ~(size_t)255));
+  int64_t n = 0;
+  auto put = [&](Request* r, int64_t m) {
+    for (int64_t t = r->next_tile; t < r->next_tile + m; t++)
+      td[n++] = {r->slot, (int32_t)(t * o.tile_rays), (int32_t)std::min<int64_t>(o.tile_rays, r->rays - t * o.tile_rays),
+                 0};
+    r->next_tile += m;
+  };
+  std::vector<int64_t> keep;
+  std::vector<Request*> large;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    for (int64_t id : unpublished) {
+      Request* r = reqs.at(id).get();
+      if (r->rays <= o.small_rays) put(r, r->ntiles - r->next_tile);
+      else large.push_back(r);
+    }
+  }
+  for (Request* r : large) {
+    while (r->next_tile < r->ntiles && backlog + n * o.tile_rays < limit)
+      put(r, std::min<int64_t>(o.publish_chunk, r->ntiles - r->next_tile));
+    if (r->next_tile < r->ntiles) keep.push_back(r->id);
+  }
+  unpublished.swap(keep);
+  if (n == 0) return;
+  // tiles, then the tail: in this order on the control stream
+  ck(cudaMemcpyAsync(tiles + tiles_published, td, n * sizeof(phx::TileDesc), cudaMemcpyHostToDevice, control),
+     "H2D tiles");
+  tiles_published += n;
+  unsigned long long* tail = reinterpret_cast<unsigned long long*>(staging + staging_bytes - 256);
+  *tail = tiles_published;
+  ck(cudaMemcpyAsync(ctl + phx::kQTail, tail, sizeof *tail, cudaMemcpyHostToDevice, control), "H2D tail");
+  ck(cudaStreamSynchronize(control), "publish");
+}
+
+// A new generation starts at the next admission (no kernel is running).
+void PhxServer::reset_queue() {
+  next_slot = 0;
+  tiles_published = 0;
+  tiles_reserved = 0;
+  unpublished.clear();
 }
 
 // Completed requests: copy results back, free their arena space.
@@ -348,8 +405,7 @@ void PhxServer::fail_inflight(const std::string& why) {
     slot_req[sl] = 0;
     inflight--;
   }
-  next_slot = 0;
-  tiles_published = 0;
+  reset_queue();
   cv_done.notify_all();
 }
 
@@ -365,10 +421,9 @@ void PhxServer::tick() {
     }
     reap();
     if (any) fail_inflight("the queue kernel left before finishing its requests (idle limit reached)");
-    next_slot = 0;
-    tiles_published = 0;
+    reset_queue();
   }
-  const bool fresh = !kernel_running && next_slot == 0 && tiles_published == 0;
+  const bool fresh = !kernel_running && next_slot == 0 && tiles_reserved == 0;
   // admissions, first in first out
   bool head_rejected = false;
   for (;;) {
@@ -385,6 +440,7 @@ void PhxServer::tick() {
     std::lock_guard<std::mutex> lk(mu);
     pending.pop_front();
   }
+  publish();
   int64_t nin;
   bool has_pending;
   {
@@ -408,8 +464,7 @@ void PhxServer::tick() {
     const double idle_ms = std::chrono::duration<double, std::milli>(Clock::now() - idle_since).count();
     if (head_rejected || (!has_pending && idle_ms >= o.linger_ms)) {
       stop_kernel();
-      next_slot = 0;
-      tiles_published = 0;
+      reset_queue();
     }
   }
 }
@@ -482,6 +537,8 @@ PhxServer* create_server(PhxSnapshot* const* snaps, int32_t nsnaps, const PhxSer
   if (o.idle_limit <= 0) o.idle_limit = 5000000;
   if (o.linger_ms < 0) o.linger_ms = 0;
   if (o.poll_us <= 0) o.poll_us = 50;
+  if (o.publish_chunk <= 0) o.publish_chunk = 64;
+  if (o.small_rays < 0) o.small_rays = 0;
   if (o.precision < PHX_PREC_FP32 || o.precision > PHX_PREC_MIXED) throw std::invalid_argument("unknown precision");
   ck(cudaGetDevice(&s->device), "cudaGetDevice");
   int64_t snap_bytes = 0;
@@ -519,6 +576,7 @@ PhxServer* create_server(PhxSnapshot* const* snaps, int32_t nsnaps, const PhxSer
   ck(cudaMemset(s->counters, 0, sizeof(unsigned long long) * phx::kNumCounters), "memset");
   ck(cudaHostAlloc((void**)&s->done_host, sizeof(int32_t) * o.max_items, cudaHostAllocMapped), "cudaHostAlloc");
   ck(cudaHostGetDevicePointer((void**)&s->done_dev, s->done_host, 0), "cudaHostGetDevicePointer");
+  ck(cudaHostAlloc((void**)&s->head_host, sizeof(unsigned long long), cudaHostAllocDefault), "cudaHostAlloc");
   // staging: descriptor | tiles of the largest request that fits the queue | tail word
   s->staging_bytes = ((s->item_bytes + 255) & ~(size_t)255) + sizeof(phx::TileDesc) * (size_t)o.max_tiles + 256;
   ck(cudaHostAlloc((void**)&s->staging, s->staging_bytes, cudaHostAllocDefault), "cudaHostAlloc staging");
@@ -555,6 +613,9 @@ void phx_default_server_options(PhxServerOptions* o) {
   o->idle_limit = 5000000;
   o->linger_ms = 20.0;
   o->poll_us = 50;
+  o->publish_chunk = 64;
+  o->backlog_rays = 0;
+  o->small_rays = 65536;
 }
 
 int phx_server_create(PhxSnapshot* const* snaps, int32_t nsnaps, const PhxServerOptions* opt, PhxServer** out) {

@@ -129,7 +129,7 @@ class PhxServerOptions(C.Structure):
         ("memory_budget", C.c_int64), ("arena_bytes", C.c_int64), ("precision", C.c_int32), ("max_freqs", C.c_int32),
         ("tile_rays", C.c_int32), ("period", C.c_int32), ("blocks_per_sm", C.c_int32), ("max_items", C.c_int32),
         ("max_tiles", C.c_int64), ("idle_ns", C.c_int32), ("idle_limit", C.c_int64), ("linger_ms", C.c_double),
-        ("poll_us", C.c_int32),
+        ("poll_us", C.c_int32), ("publish_chunk", C.c_int32), ("backlog_rays", C.c_int64), ("small_rays", C.c_int64),
     ]
 
 

@@ -100,3 +100,24 @@ def test_kernel_restarts_after_idle(snaps):
         st = srv.stats()
     assert st["generations"] >= 2
     assert np.array_equal(a, b)
+
+
+def test_small_request_overtakes_a_large_one(snaps):
+    """A small request enters the queue whole, ahead of the rest of a large one that is published a chunk at a time:
+    submitted right after the large one, it finishes first, and both results stay the ones each gets alone."""
+    big_p = _params("cfg1", "fp32", img_width=256, img_height=256)
+    small_p = _params("edge", "fp32")
+    with P.Server(snaps, "fp32", max_freqs=1, backlog_rays=4096, publish_chunk=16, small_rays=1024) as srv:
+        big = srv.submit(0, big_p)
+        small = srv.submit(1, small_p)
+        srv.wait(small, WAIT)
+        srv.wait(big, WAIT)
+        rs, ts = srv.result(small)
+        rb, tb = srv.result(big)
+        alone = srv.submit(1, small_p)
+        srv.wait(alone, WAIT)
+        ra, _ = srv.result(alone)
+    assert ts["submitted_s"] + ts["done_s"] < tb["submitted_s"] + tb["done_s"]
+    assert np.array_equal(rs, ra)
+    single, _ = snaps[0].render(big_p)
+    assert flux_errors(rb, single, big_p).max() <= 1e-5
