@@ -288,8 +288,8 @@ def run_batch(args):
     ms = min(t_plain)
     line["plain_fp32"] = {"ms": ms, "ray_steps_per_s": steps / (ms * 1e-3), "images_per_s": len(imgs) / (ms * 1e-3),
                           "launches": len(imgs)}
-    fluxes = {}
-    for prec in ("fp32", "mixed", "fp64"):
+    ref_images = []
+    for prec in ("fp64", "fp32", "mixed"):
         items = [(snap, P.make_params(precision=prec, **im)) for im in imgs]
         t0 = time.time()
         b = P.Batch(items, autotune=not args.no_autotune)
@@ -298,24 +298,28 @@ def run_batch(args):
         tune = b.tuning()
         ms = min(ts)
         bsteps = 0
-        fl = []
+        errs = []
         for k in range(len(items)):
             res, info = b.result(k)
             bsteps += info["steps"]
-            fl.append(P.flux(res, items[k][1])[0])
-        fluxes[prec] = np.array(fl)
+            if prec == "fp64":
+                ref_images.append(res)
+            else:
+                errs.append(image_errors(res, ref_images[k], items[k][1]))
         line["batch_" + prec] = {"ms": ms, "ray_steps_per_s": bsteps / (ms * 1e-3),
                                  "images_per_s": len(imgs) / (ms * 1e-3), "launches": 2,
                                  "create_s": create_s, "tuning": {k: tune[k] for k in
                                                                   ("blocks_per_sm", "period", "tile_rays", "grid",
                                                                    "regs", "ntiles", "device_bytes")},
                                  "candidates": tune["candidates"], "ray_steps": bsteps}
+        if errs:
+            fI = np.array([e["flux_I"] for e in errs])
+            line["batch_" + prec]["errors_vs_fp64"] = {
+                "flux_I_max": float(fI.max()), "flux_I_median": float(np.median(fI)),
+                "images_flux_I_over_1e-4": int((fI > 1e-4).sum()),
+                "flux_QUV_max": float(max(e["flux_QUV"] for e in errs)),
+                "l1_I_max": float(max(e["l1_I"] for e in errs)), "linf_I_max": float(max(e["linf_I"] for e in errs))}
         b.close()
-    ref = fluxes["fp64"]
-    for prec in ("fp32", "mixed"):
-        err = np.abs(fluxes[prec] - ref) / np.abs(ref[:, :1])
-        line["batch_" + prec]["flux_err_vs_fp64"] = {"I_max": float(err[:, 0].max()),
-                                                     "QUV_max": float(err[:, 1:].max())}
     pl = line["plain_fp32"]["ray_steps_per_s"]
     line["speedup_vs_plain_fp32"] = {p: line["batch_" + p]["ray_steps_per_s"] / pl for p in ("fp32", "mixed", "fp64")}
     snap.close()
@@ -481,6 +485,78 @@ def run_reference_gpu(args):
     print(json.dumps(line), flush=True)
 
 
+def image_errors(res, ref, params):
+    """Per-frequency total-flux error relative to Stokes I, and per-pixel L1 / Linf of I relative to the image's I."""
+    import phoenix_b200 as P
+    f, g = P.flux(res, params), P.flux(ref, params)
+    ferr = np.abs(f - g) / np.abs(g[:, :1])
+    I, Iref = res[..., 0], ref[..., 0]
+    ok = np.isfinite(I) & np.isfinite(Iref)
+    d = np.abs(np.where(ok, I - Iref, 0.0))
+    return {"flux_I": float(ferr[:, 0].max()), "flux_QUV": float(ferr[:, 1:].max()),
+            "l1_I": float(d.sum() / np.abs(np.where(ok, Iref, 0.0)).sum()),
+            "linf_I": float(d.max() / np.abs(np.where(ok, Iref, 0.0)).max())}
+
+
+# Mixed-precision workload: the plain-path generator at seed 1, 1024^2 and 2048^2 images, three frequencies, m_unit 1e19
+# (optically and Faraday thick regions).
+MIXED = dict(seed=1, images=(1024, 2048), frequencies=(86e9, 230e9, 345e9), m_unit=1e19, inclination=60.0)
+
+
+def run_mixed(args):
+    """Config 3: FP32, mixed and FP64 renders of the same images; per-image flux and per-pixel errors of FP32 and mixed
+    against the FP64 path (itself pinned to the FP64 oracle on the parity cases), and device times.  Prints one line."""
+    import torch
+
+    import phoenix_b200 as P
+    w = dict(WORKLOAD)
+    w["seed"] = MIXED["seed"]
+    dump, grid = snapshot_files(w)
+    snap = P.Snapshot.load(dump, grid, nlevels=w["nlevels"], f64_prims=True)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    out = {"workload": "mixed", "config": {"snapshot": "192x96x96 base grid, 8^3 blocks, 3 AMR levels, seed 1",
+                                           "frequencies": list(MIXED["frequencies"]), "m_unit": MIXED["m_unit"],
+                                           "inclination": MIXED["inclination"]}, "images": []}
+    for side in MIXED["images"]:
+        npix = side * side
+        jobs = torch.from_numpy(P.schedule_morton(side, side)).to(dev)
+        nf = len(MIXED["frequencies"])
+        row = {"image": side}
+        results = {}
+        for prec in ("fp64", "fp32", "mixed"):
+            p = P.make_params(precision=prec, img=side, frequencies=list(MIXED["frequencies"]),
+                              m_unit=MIXED["m_unit"], inclination=MIXED["inclination"])
+            res = torch.zeros((npix, nf, 6), dtype=torch.float64, device=dev)
+            ctr = torch.zeros(P.NUM_COUNTERS, dtype=torch.int64, device=dev)
+            best = None
+            for r in range(2):
+                with torch.cuda.stream(stream):
+                    flush.fill_(r)
+                    ctr.zero_()
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    snap.render_async(p, jobs.data_ptr(), npix, res.data_ptr(), ctr.data_ptr(), 0, stream.cuda_stream)
+                    e1.record(stream)
+                stream.synchronize()
+                ms = e0.elapsed_time(e1)
+                best = ms if best is None else min(best, ms)
+            steps = int(ctr[P.CTR["steps"]])
+            row[prec] = {"ms": best, "ray_steps_per_s": steps / (best * 1e-3),
+                         "fp64_steps": int(ctr[P.CTR["fp64_steps"]]), "fp64_ops": int(ctr[P.CTR["fp64_ops"]])}
+            # FreqOut index (i * H + j) * F + f: the device buffer is in pixel order already
+            results[prec] = (res.cpu().numpy().reshape(side, side, nf, 6), p)
+        ref = results["fp64"][0]
+        for prec in ("fp32", "mixed"):
+            row[prec]["errors_vs_fp64"] = image_errors(results[prec][0], ref, results[prec][1])
+        row["speed_mixed_vs_fp32"] = row["mixed"]["ray_steps_per_s"] / row["fp32"]["ray_steps_per_s"]
+        row["speed_mixed_vs_fp64"] = row["mixed"]["ray_steps_per_s"] / row["fp64"]["ray_steps_per_s"]
+        out["images"].append(row)
+    snap.close()
+    print(json.dumps(out), flush=True)
+
+
 def run_ingest(args):
     """Snapshot admission: the plain-path workload's dump read and made resident with the host decode (16 OpenMP
     threads on the GPU box) and with the GPU decode (cells decoded on the device while the dump streams in).  The dump
@@ -516,7 +592,7 @@ def main():
     ap.add_argument("--period", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="plain", choices=["plain", "batch", "serve", "ingest"],
+    ap.add_argument("--workload", default="plain", choices=["plain", "batch", "serve", "ingest", "mixed"],
                     help="plain: the headline single-image path (default); batch: the 128-image sweep; "
                          "serve: Poisson request streams through the server")
     ap.add_argument("--requests", type=int, default=0, help="serve: requests per stream")
@@ -533,6 +609,8 @@ def main():
         return run_serve(args)
     if args.workload == "ingest":
         return run_ingest(args)
+    if args.workload == "mixed":
+        return run_mixed(args)
 
     import torch
     import torch.distributed as dist
