@@ -99,7 +99,7 @@ PHX_HD KerrPt<T> kerr_point_r(T a, T hs, T r, T x2) {
   }
   p.s2 = p.s * p.s;
   p.sig = p.r * p.r + a * a * p.c * p.c;
-  p.isig = T(1) / p.sig;
+  p.isig = fastm::rcp(p.sig);  // FP32: hardware reciprocal (2 ulp), FP64: exact division
   p.q = T(2) * p.r * p.isig;
   return p;
 }
@@ -127,9 +127,9 @@ template <class T>
 PHX_HD Contra<T> contra_metric(const KerrPt<T>& p, T a) {
   Contra<T> u;
   const T isig = p.isig;
-  const T ir = T(1) / p.r;
+  const T ir = fastm::rcp(p.r);
   const T tp2 = p.tp * p.tp;
-  const T iprod = isig / (tp2 * p.s2);  // one division for both 1 / theta'^2 and 1 / sin^2
+  const T iprod = isig * fastm::rcp(tp2 * p.s2);  // one reciprocal for both 1 / theta'^2 and 1 / sin^2
   u.tt = -(T(1) + p.q);
   u.t1 = T(2) * isig;
   u.x11 = isig * ((p.r - T(2)) * p.r + a * a) * ir * ir;
