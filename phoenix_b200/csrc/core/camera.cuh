@@ -102,15 +102,15 @@ PHX_HD void camera_photon(const CameraSpec& cs, double alpha, double beta, doubl
 template <class R>
 PHX_HD void observer_axes_lowered(R sqrtg, const R k[4], const R U[4], const R b[4], const R kd[4], const R Ud[4],
                                   const R bd[4], R omega, R kb, R Ub, R bb, R perp[4], R para[4]) {
-  const R iomega = R(1) / omega;
+  const R iomega = fastm::rcp(omega);
   R eK[4];
   for (int i = 0; i < 4; i++) eK[i] = k[i] * iomega - U[i];
   const R Beta = Ub;
   const R Cc = kb * iomega - Beta;
   const R Nc = sqrt_t(bb + Beta * Beta - Cc * Cc);
-  const R iNc = R(1) / Nc;
+  const R iNc = fastm::rcp(Nc);
   for (int i = 0; i < 4; i++) para[i] = (b[i] + Beta * U[i] - Cc * eK[i]) * iNc;
-  const R s = -iomega * iNc / sqrtg;
+  const R s = -iomega * iNc * fastm::rcp(sqrtg);
   // generalized cross product: perp^i = (-1)^i det[U, k, b] over the three columns other than i
   const R m01 = kd[0] * bd[1] - kd[1] * bd[0], m02 = kd[0] * bd[2] - kd[2] * bd[0], m03 = kd[0] * bd[3] - kd[3] * bd[0];
   const R m12 = kd[1] * bd[2] - kd[2] * bd[1], m13 = kd[1] * bd[3] - kd[3] * bd[1], m23 = kd[2] * bd[3] - kd[3] * bd[2];

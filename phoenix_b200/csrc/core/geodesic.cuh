@@ -168,11 +168,11 @@ template <class R>
 PHX_HD R step_size_fast(R stepsize, R inv_stepsize, R x2, const R k[4], const R* idxc, R tiny, R big) {
   const R a1 = fabs_t(k[1]) + tiny, a2 = fabs_t(k[2]) + tiny, a3 = fabs_t(k[3]) + tiny;
   const R m = fmin_t(x2, R(kPi) - x2);
-  const R i2 = fmin_t(a2 / (stepsize * m), R(1) / tiny);  // m = 0 (or underflow): the reference's 1 / tiny
+  const R i2 = fmin_t(fastm::div(a2, stepsize * m), R(1) / tiny);  // m = 0 (or underflow): the reference's 1 / tiny
   const R sum = (a1 + a3) * inv_stepsize + i2;
   R grid = big;
-  if (idxc) grid = R(0.25) / (a1 * idxc[0] + a2 * idxc[1] + a3 * idxc[2]);
-  return -fmin_t(R(1) / sum, grid);
+  if (idxc) grid = fastm::div(R(0.25), a1 * idxc[0] + a2 * idxc[1] + a3 * idxc[2]);
+  return -fmin_t(fastm::rcp(sum), grid);
 }
 
 // Re-solve k^t from the spatial components so that g_{mu nu} k^mu k^nu = 0 (the larger root), as the reference

@@ -283,7 +283,7 @@ struct Ray {
     const R Bn = sqrt_t(fabs_t(BB));
     R sth = R(1), cth = R(0);
     if (Bn != R(0)) {
-      R mu = kB / (fabs_t(kU) * Bn);
+      R mu = fastm::div(kB, fabs_t(kU) * Bn);
       if (fabs_t(mu) > R(1)) mu /= fabs_t(mu);
       if (mu == R(1) || mu == R(-1)) return;
       sth = sqrt_t((R(1) - mu) * (R(1) + mu));
@@ -294,7 +294,7 @@ struct Ray {
     observer_axes_lowered(sqrt_neg_g(p), k, fl.U, fl.B, kd, Ud, Bd, -kU, kB, UB, BB, perp, para);
     symv(g, pF, pFd);
     const R C = dot4(pFd, perp), S = dot4(pFd, para);
-    const R inn = R(1) / (C * C + S * S);
+    const R inn = fastm::rcp(C * C + S * S);
     const R c2 = (C * C - S * S) * inn, s2 = R(2) * C * S * inn;
     const R ratio = -kU;  // nu_plasma / nu_camera
     const SynchroSample<R> ss = synchro_sample(fl.theta_e, fl.n_e, fl.Bmag, sth, cth);

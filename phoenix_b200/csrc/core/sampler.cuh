@@ -181,7 +181,7 @@ PHX_HD void cell_weights(const SnapView<R, PT>& s, int leaf, const R x[4], int c
   for (int d = 0; d < 3; d++) {
     const R lb = ldg(s.lb + 3 * leaf + d), dx = ldg(s.dxc + 3 * leaf + d);
     // FP32: one reciprocal per axis (rounding-level difference; the interpolant is continuous across cells)
-    const R idx = sizeof(R) == 4 ? R(1) / dx : R(0);
+    const R idx = sizeof(R) == 4 ? fastm::rcp(dx) : R(0);
     const R u = sizeof(R) == 4 ? (x[1 + d] - lb) * idx : (x[1 + d] - lb) / dx;
     c[d] = (int)u;
     if (c[d] >= s.nx[d]) c[d] = s.nx[d] - 1;
@@ -259,12 +259,12 @@ PHX_HD bool derive_fluid(const PlasmaView<R>& pv, R gam, R r, const Cov<R>& g, c
   fl->n_e = rho * pv.Ne + smalll;
   // lapse alpha = 1 / sqrt(-g^tt), shift^1 = alpha^2 g^t1; the divisions are folded into reciprocals
   const R ialpha = sqrt_t(-u.tt);
-  const R alpha = R(1) / ialpha;
+  const R alpha = fastm::rcp(ialpha);  // FP32: hardware reciprocals and quotients here (2 ulp); FP64: exact
   const R shift1 = u.t1 * alpha * alpha;
   const R gv1 = q[kU1], gv2 = q[kU2], gv3 = q[kU3];
   const R gvv = g.x11 * gv1 * gv1 + R(2) * g.x13 * gv1 * gv3 + g.x22 * gv2 * gv2 + g.x33 * gv3 * gv3;
   const R lfac = sqrt_t(gvv + R(1));
-  const R ilfac = R(1) / lfac;
+  const R ilfac = fastm::rcp(lfac);
   const R V1 = gv1 * ilfac, V2 = gv2 * ilfac, V3 = gv3 * ilfac;
   const R ut = lfac * ialpha;
   fl->U[0] = ut;
@@ -280,13 +280,14 @@ PHX_HD bool derive_fluid(const PlasmaView<R>& pv, R gam, R r, const Cov<R>& g, c
   fl->B[3] = (Bp3 + alpha * fl->B[0] * fl->U[3]) * ilfac;
   const R Bsq = fabs_t(dot(g, fl->B, fl->B)) + smalll;
   fl->Bmag = sqrt_t(Bsq) * pv.Bu;
-  const R beta = uu * (gam - R(1)) / (R(0.5) * (Bsq + smalll));
+  const R beta = fastm::div(uu * (gam - R(1)), R(0.5) * (Bsq + smalll));
   const R bb = beta * pv.ibc;
   const R b2 = bb * bb;
-  const R trat = pv.rhigh * b2 / (R(1) + b2) + pv.rlow / (R(1) + b2);
-  const R te_unit = R(1.0 / 3.0 * (cgs::m_proton / cgs::m_electron)) / (trat + R(1));
-  fl->theta_e = (uu / rho) * te_unit;
-  if ((Bsq / (rho + R(1e-20)) > pv.sigma_cut) || r > pv.rt_outer || fl->theta_e > pv.thetae_max ||
+  const R ib2 = fastm::rcp(R(1) + b2);
+  const R trat = (pv.rhigh * b2 + pv.rlow) * ib2;
+  const R te_unit = fastm::div(R(1.0 / 3.0 * (cgs::m_proton / cgs::m_electron)), trat + R(1));
+  fl->theta_e = fastm::div(uu, rho) * te_unit;
+  if ((fastm::div(Bsq, rho + R(1e-20)) > pv.sigma_cut) || r > pv.rt_outer || fl->theta_e > pv.thetae_max ||
       fl->theta_e < pv.thetae_min) {
     fl->n_e = R(0);
     return false;
