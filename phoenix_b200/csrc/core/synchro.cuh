@@ -86,7 +86,7 @@ PHX_HD void bessel_ratios(R x, R* r10, R* r02) {
     if (x >= T[q].a) p = q;
   const BesselPiece<R>* pc = T + p;
   const R la = pc->la, lb = pc->lb;
-  const R z = (R(2) * log_t(x) - (lb + la)) / (lb - la);
+  const R z = fastm::div(R(2) * log_t(x) - (lb + la), lb - la);
   const int n = sizeof(R) == 4 ? pc->n32 : pc->n64;
   R b1a = R(0), b2a = R(0), b1b = R(0), b2b = R(0);
   for (int j = n - 1; j >= 1; j--) {
@@ -125,14 +125,14 @@ PHX_HD SynchroSample<R> synchro_sample(R te, R ne, R B, R sth, R cth) {
   s.sth = sth;
   s.cth = cth;
   s.te = te;
-  s.ite = R(1) / te;
+  s.ite = fastm::rcp(te);
   s.inu_c = fastm::div(R(1), R(NU_CRIT) * B * s.sth * te * te);
   s.jpre = R(JNU) * ne * s.ite * s.ite;
   if (s.ite < R(1.0 / 5.0)) {
     // Theta_e > 5: K_nu(x) -> 2^(nu-1) (nu-1)! x^-nu (nu > 0), K_0 -> -ln(x/2) - gamma_E
-    const R k0 = -log_t(s.ite / R(2)) - R(0.5772), k1 = R(1) / s.ite, k2 = R(2) / s.ite / s.ite;
-    s.kr1 = k1 / k2;
-    s.kr0 = (k2 > R(0)) ? k0 / k2 : R(1);
+    const R k0 = -log_t(s.ite * R(0.5)) - R(0.5772), k1 = fastm::rcp(s.ite), k2 = R(2) * k1 * k1;
+    s.kr1 = fastm::div(k1, k2);
+    s.kr0 = (k2 > R(0)) ? fastm::div(k0, k2) : R(1);
   } else {
     bessel_ratios(s.ite, &s.kr1, &s.kr0);
   }
@@ -168,7 +168,8 @@ PHX_HD Coeffs<R> synchro_coeffs(const SynchroSample<R>& s, R nu, R jscale) {
   R jQ = pref * IQ;
   R jV = R(4.0 / 3.0) * pref * s.ite * fastm::div(s.cth, s.sth) * IV;
   // Kirchhoff: alpha = j / B_nu(Theta_e)
-  const R pre = R(2.0 * cgs::h_planck) * nu * nu * nu / R(cgs::c_light * cgs::c_light);
+  // (2 h nu^3) / c^2 in this order: 2 h / c^2 alone (1.5e-47) is below the FP32 range
+  const R pre = R(2.0 * cgs::h_planck) * nu * nu * nu * R(1.0 / (cgs::c_light * cgs::c_light));
   const R xx = R(H_OVER_MEC2) * nu * s.ite;
   const R iB = fastm::div(sizeof(R) == 4 ? expm1_t(xx) : (exp_t(xx) - R(1)), pre);
   R aI = jI * iB, aQ = jQ * iB, aV = jV * iB;
