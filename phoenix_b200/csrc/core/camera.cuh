@@ -107,7 +107,7 @@ PHX_HD void observer_axes_lowered(R sqrtg, const R k[4], const R U[4], const R b
   for (int i = 0; i < 4; i++) eK[i] = k[i] * iomega - U[i];
   const R Beta = Ub;
   const R Cc = kb * iomega - Beta;
-  const R Nc = sqrt_t(bb + Beta * Beta - Cc * Cc);
+  const R Nc = fastm::sqrt(bb + Beta * Beta - Cc * Cc);
   const R iNc = fastm::rcp(Nc);
   for (int i = 0; i < 4; i++) para[i] = (b[i] + Beta * U[i] - Cc * eK[i]) * iNc;
   const R s = -iomega * iNc * fastm::rcp(sqrtg);

@@ -126,6 +126,10 @@ PHX_D float exp(float x) { return __expf(x); }
 PHX_D float log(float x) { return __logf(x); }
 PHX_D float div(float a, float b) { return __fdividef(a, b); }
 PHX_D float rcp(float x) { return __fdividef(1.0f, x); }
+// sqrt from the hardware reciprocal square root (about 2 ulp): NaN for x < 0 like sqrtf (a bad sample stays bad),
+// 0 at x = 0 (where x * rsqrt(x) would be 0 * inf)
+PHX_D float sqrt(float x) { return x == 0.0f ? 0.0f : x * rsqrtf(x); }
+PHX_D float rsqrt(float x) { return rsqrtf(x); }
 PHX_D float tanh(float x) { return 1.0f - __fdividef(2.0f, __expf(2.0f * x) + 1.0f); }
 PHX_D float cos(float x) { return __cosf(x); }
 #else
@@ -133,6 +137,8 @@ inline float exp(float x) { return std::exp(x); }
 inline float log(float x) { return std::log(x); }
 inline float div(float a, float b) { return a / b; }
 inline float rcp(float x) { return 1.0f / x; }
+inline float sqrt(float x) { return std::sqrt(x); }
+inline float rsqrt(float x) { return 1.0f / std::sqrt(x); }
 inline float tanh(float x) { return std::tanh(x); }
 inline float cos(float x) { return std::cos(x); }
 #endif
@@ -140,6 +146,8 @@ PHX_HD double exp(double x) { return exp_t(x); }
 PHX_HD double log(double x) { return log_t(x); }
 PHX_HD double div(double a, double b) { return a / b; }
 PHX_HD double rcp(double x) { return 1.0 / x; }
+PHX_HD double sqrt(double x) { return sqrt_t(x); }
+PHX_HD double rsqrt(double x) { return 1.0 / sqrt_t(x); }
 PHX_HD double tanh(double x) { return tanh_t(x); }
 PHX_HD double cos(double x) { return cos_t(x); }
 }  // namespace fastm

@@ -280,13 +280,13 @@ struct Ray {
     const R kU = dot4(kd, fl.U), kB = dot4(kd, fl.B), UB = dot4(Ud, fl.B), BB = dot4(Bd, fl.B);
     // pitch angle of k to B in the plasma frame (tetrad.hpp:138-154): only its sine and cosine enter the
     // coefficients, so they are formed from mu = cos(pitch) directly; acos(mu) is 0 or pi exactly when mu = +-1
-    const R Bn = sqrt_t(fabs_t(BB));
+    const R Bn = fastm::sqrt(fabs_t(BB));
     R sth = R(1), cth = R(0);
     if (Bn != R(0)) {
       R mu = fastm::div(kB, fabs_t(kU) * Bn);
       if (fabs_t(mu) > R(1)) mu /= fabs_t(mu);
       if (mu == R(1) || mu == R(-1)) return;
-      sth = sqrt_t((R(1) - mu) * (R(1) + mu));
+      sth = fastm::sqrt((R(1) - mu) * (R(1) + mu));
       cth = mu;
     }
     // polarization axes of the plasma frame with B as reference direction; EVPA rotation from the transported F1

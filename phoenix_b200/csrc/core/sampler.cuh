@@ -258,12 +258,12 @@ PHX_HD bool derive_fluid(const PlasmaView<R>& pv, R gam, R r, const Cov<R>& g, c
   const R rho = q[kRho], uu = q[kUU];
   fl->n_e = rho * pv.Ne + smalll;
   // lapse alpha = 1 / sqrt(-g^tt), shift^1 = alpha^2 g^t1; the divisions are folded into reciprocals
-  const R ialpha = sqrt_t(-u.tt);
+  const R ialpha = fastm::sqrt(-u.tt);
   const R alpha = fastm::rcp(ialpha);  // FP32: hardware reciprocals and quotients here (2 ulp); FP64: exact
   const R shift1 = u.t1 * alpha * alpha;
   const R gv1 = q[kU1], gv2 = q[kU2], gv3 = q[kU3];
   const R gvv = g.x11 * gv1 * gv1 + R(2) * g.x13 * gv1 * gv3 + g.x22 * gv2 * gv2 + g.x33 * gv3 * gv3;
-  const R lfac = sqrt_t(gvv + R(1));
+  const R lfac = fastm::sqrt(gvv + R(1));
   const R ilfac = fastm::rcp(lfac);
   const R V1 = gv1 * ilfac, V2 = gv2 * ilfac, V3 = gv3 * ilfac;
   const R ut = lfac * ialpha;
@@ -279,7 +279,7 @@ PHX_HD bool derive_fluid(const PlasmaView<R>& pv, R gam, R r, const Cov<R>& g, c
   fl->B[2] = (Bp2 + alpha * fl->B[0] * fl->U[2]) * ilfac;
   fl->B[3] = (Bp3 + alpha * fl->B[0] * fl->U[3]) * ilfac;
   const R Bsq = fabs_t(dot(g, fl->B, fl->B)) + smalll;
-  fl->Bmag = sqrt_t(Bsq) * pv.Bu;
+  fl->Bmag = fastm::sqrt(Bsq) * pv.Bu;
   const R beta = fastm::div(uu * (gam - R(1)), R(0.5) * (Bsq + smalll));
   const R bb = beta * pv.ibc;
   const R b2 = bb * bb;

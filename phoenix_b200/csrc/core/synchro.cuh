@@ -162,7 +162,7 @@ PHX_HD Coeffs<R> synchro_coeffs(const SynchroSample<R>& s, R nu, R jscale) {
   const R pref = s.jpre * nu;
   const R II = R(2.5651) * (R(1) + R(1.92) * icx + R(0.9977) * icx * icx) * ex;
   const R IQ = R(2.5651) * (R(1) + R(0.93193) * icx + R(0.499873) * icx * icx) * ex;
-  const R IV = (R(1.81348) * icx * icx * icx + R(3.42319) * icx * icx + fastm::div(R(0.0292545), sqrt_t(x)) +
+  const R IV = (R(1.81348) * icx * icx * icx + R(3.42319) * icx * icx + R(0.0292545) * fastm::rsqrt(x) +
                 R(2.03773) * icx) * ex;
   R jI = pref * II;
   R jQ = pref * IQ;
@@ -175,7 +175,7 @@ PHX_HD Coeffs<R> synchro_coeffs(const SynchroSample<R>& s, R nu, R jscale) {
   R aI = jI * iB, aQ = jQ * iB, aV = jV * iB;
   // Faraday rotation / conversion
   const R iw = fastm::div(R(1), R(kTwoPi) * nu);
-  const R Xe = s.te * sqrt_t(R(1.4142135623730951) * s.sth * fastm::div(R(1e3 / kTwoPi) * s.omega0, nu));
+  const R Xe = s.te * fastm::sqrt(R(1.4142135623730951) * s.sth * fastm::div(R(1e3 / kTwoPi) * s.omega0, nu));
   const R lx = fastm::log(Xe);
   const R exm = fastm::exp(-Xe * R(1.0 / 47.2));
   const R fm = R(2.011) * fastm::exp(-fastm::exp(R(1.035) * lx) * R(1.0 / 4.7)) -
@@ -198,7 +198,7 @@ PHX_HD Coeffs<R> synchro_coeffs(const SynchroSample<R>& s, R nu, R jscale) {
   aV *= nu;
   rQ *= nu;
   rV *= nu;
-  const R pf = fastm::div(sqrt_t(jQ * jQ + jV * jV), jI);
+  const R pf = fastm::div(fastm::sqrt(jQ * jQ + jV * jV), jI);
   if (pf > R(1)) {
     const R ipf = fastm::div(R(1), pf + R(0.005));
     jQ *= ipf;
