@@ -236,6 +236,41 @@ def batch_images(b=BATCH):
 
 
 def run_batch(args):
+    if args.batch_images:
+        return run_batch_small(args)
+    return run_batch_sweep(args)
+
+
+def run_batch_small(args):
+    """A small FP32 batch (the first N images of the sweep, all at 256^2): one graph launch per step, for profiling
+    the queue kernel on a case that ncu can capture quickly."""
+    import torch
+
+    import phoenix_b200 as P
+    dev = torch.device("cuda", 0)
+    dump, grid = generated_snapshot(BATCH["gen"])
+    snap = P.Snapshot.load(dump, grid, nlevels=BATCH["nlevels"])
+    imgs = [dict(im, img=256) for im in batch_images()[:args.batch_images]]
+    stream = torch.cuda.Stream(device=dev)
+    b = P.Batch([(snap, P.make_params(precision="fp32", **im)) for im in imgs], blocks_per_sm=3, period=32)
+    ts = []
+    for r in range(max(1, args.warmup) + max(1, args.steps)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            b.launch(stream.cuda_stream)
+            e1.record(stream)
+        stream.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    steps = sum(b.result(k)[1]["steps"] for k in range(len(imgs)))
+    ms = min(ts[max(1, args.warmup):])
+    print(json.dumps({"workload": "batch-small", "images": len(imgs), "ms": ms, "ray_steps": steps,
+                      "ray_steps_per_s": steps / (ms * 1e-3), "tuning": b.tuning()["regs"]}), flush=True)
+    b.close()
+    snap.close()
+
+
+def run_batch_sweep(args):
     """Config 4: the 128-image sweep rendered one by one with the plain single-image path (FP32) and as one batch
     (FP32, mixed and FP64; autotuned launch shape).  Device-resident inputs, CUDA-event timing, L2 flushed between
     timed repetitions.  Prints one JSON line."""
@@ -598,6 +633,7 @@ def main():
     ap.add_argument("--requests", type=int, default=0, help="serve: requests per stream")
     ap.add_argument("--rates", type=float, nargs="*", default=None, help="serve: arrival rates [1/s]")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--batch-images", type=int, default=0, help="batch: a small 256^2 batch of this many images")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
