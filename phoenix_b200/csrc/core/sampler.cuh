@@ -30,6 +30,7 @@ struct SnapView {
   int32_t nx[3];
   R x_lo[4], x_hi[4];
   R w0[3];  // base-level block widths
+  R iw0up[3];  // finest-level slots per unit of x: 2^(nlevels-1) / w0
   R a, hs, gam;
   // FP64 leaf geometry, used by the mixed-precision path to place FP32 samples in leaves and cells exactly
   const double* lbd;
@@ -46,6 +47,7 @@ struct SnapView {
       v.fd[d] = fd[d];
       v.nx[d] = nx[d];
       v.w0[d] = w0_d[d];
+      v.iw0up[d] = double(1 << (nlevels - 1)) / w0_d[d];
     }
     for (int d = 0; d < 4; d++) {
       v.x_lo[d] = xlo_d[d];
@@ -99,12 +101,21 @@ PHX_HD R leaf_nudge(const R x[4]) {
   return x[2] > R(kHalfPi) ? R(-1e-9) : R(1e-9);
 }
 
+// fast: slot coordinates from the precomputed scale instead of the divisions (FP32; the caller verifies the
+// candidate and retries with the divisions, so the leaf found is the same)
 template <class R, class PT>
-PHX_HD int find_leaf_map(const SnapView<R, PT>& s, const R x[4], R small) {
+PHX_HD int find_leaf_map(const SnapView<R, PT>& s, const R x[4], R small, bool fast = false) {
   const R up = R(1 << (s.nlevels - 1));
-  const R fi = (x[1] + small - s.x_lo[1]) / s.w0[0] * up;
-  const R fj = (x[2] + small - s.x_lo[2]) / s.w0[1] * up;
-  const R fk = (x[3] + small - s.x_lo[3]) / s.w0[2] * up;
+  R fi, fj, fk;
+  if (fast) {
+    fi = (x[1] + small - s.x_lo[1]) * s.iw0up[0];
+    fj = (x[2] + small - s.x_lo[2]) * s.iw0up[1];
+    fk = (x[3] + small - s.x_lo[3]) * s.iw0up[2];
+  } else {
+    fi = (x[1] + small - s.x_lo[1]) / s.w0[0] * up;
+    fj = (x[2] + small - s.x_lo[2]) / s.w0[1] * up;
+    fk = (x[3] + small - s.x_lo[3]) / s.w0[2] * up;
+  }
   if (fi < R(0) || fj < R(0) || fk < R(0)) return -1;
   const int i = (int)fi, j = (int)fj, k = (int)fk;
   if (i >= s.fd[0] || j >= s.fd[1] || k >= s.fd[2]) return -1;
@@ -162,8 +173,12 @@ PHX_HD_OUTLINE int find_leaf_scan(const SnapView<R, PT>& s, R x1, R x2, R x3, R 
 template <class R, class PT>
 PHX_HD int find_leaf(const SnapView<R, PT>& s, const R x[4], bool* scanned) {
   const R small = leaf_nudge(x);
-  const int cand = find_leaf_map(s, x, small);
+  int cand = find_leaf_map(s, x, small, sizeof(R) == 4);
   if (cand >= 0 && inside_leaf(s, cand, x, small)) return cand;
+  if constexpr (sizeof(R) == 4) {
+    cand = find_leaf_map(s, x, small);
+    if (cand >= 0 && inside_leaf(s, cand, x, small)) return cand;
+  }
   const R eps = R(1e-6);
   if (cand < 0 && (x[1] < s.x_lo[1] - eps || x[1] > s.x_hi[1] + eps || x[2] < s.x_lo[2] - eps ||
                    x[2] > s.x_hi[2] + eps || x[3] < s.x_lo[3] - eps || x[3] > s.x_hi[3] + eps))

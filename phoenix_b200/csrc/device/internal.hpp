@@ -110,6 +110,7 @@ phx::SnapView<R, PT> snap_view(const PhxSnapshot* s, const R* lb, const R* dxc, 
     v.x_lo[1 + d] = R(s->x_lo[d]);
     v.x_hi[1 + d] = R(s->x_hi[d]);
     v.w0[d] = R((s->x_hi[d] - s->x_lo[d]) / s->ng[d]);
+    v.iw0up[d] = R(double(1 << (s->nlevels - 1)) * s->ng[d] / (s->x_hi[d] - s->x_lo[d]));
   }
   v.x_lo[0] = v.x_hi[0] = R(0);
   v.nleafs = s->nleafs;
