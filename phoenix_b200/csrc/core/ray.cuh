@@ -1,8 +1,9 @@
 // One ray of the raymarch as a resumable state machine.
 //
-// Ray::advance() performs exactly one pass of the reference's per-pixel loop (core/render/pixel.hpp:179-211):
-//   view the state -> liveness test -> process the PREVIOUS sample with the sampler cache seeded by this sample's
-//   leaf -> theta turning points -> grid-capped step size -> RK4 step.
+// Ray::advance() performs one pass of the reference's per-pixel loop (core/render/pixel.hpp:179-211): view the
+// state -> liveness test -> leaf lookup -> a plasma sample -> theta turning points -> grid-capped step size -> RK4
+// step.  FP64 processes the previous point's sample, as the reference does; the FP32 paths process this point's
+// (see advance() for why both give the same samples).
 // Because the state is explicit, a warp can retire a finished ray and start a new one in the same lane while its
 // neighbours keep marching (the kernel's lane refill), instead of idling until the warp's longest ray ends.
 //
@@ -94,10 +95,10 @@ struct Ray {
   using Pol = Policy<M>;
   using R = typename Pol::R;
   static constexpr bool kComp = Pol::kComp, kMixed = Pol::kMixed;
+  static constexpr bool kLate = M == Mode::kFP64;  // the reference's one-pass-late sample order (see advance())
 
   GeoState<R> geo;
-  R px[4], pk[4], pF[4], pdl;
-  std::conditional_t<kMixed, double, char> pxd[4];  // mixed: the pending sample's compensated position in FP64
+  R px[4], pk[4], pF[4], pdl;  // FP64 (kLate): the pending sample's point and the length of the step to it
   bool pvalid, terminate;
   int steps, turns, bsign, nplasma, bad;
   R thdot_prev, dl_prev;
@@ -123,7 +124,31 @@ struct Ray {
     idxc[0] = idxc[1] = idxc[2] = R(0);
   }
 
-  // One pass of the march loop; false once the ray has ended (its pending sample has then been processed).
+  // The leaf of the wrapped point xw (the last one first: a ray stays tens of steps in one leaf, and since the
+  // leaves tile the domain a point inside it has no other leaf); -1 outside the domain.  Also keeps the leaf's
+  // inverse cell sizes for the FP32 step-size cap.
+  PHX_HD int lookup(const SnapView<R, PT>& s, const R xw[4], RayCounters& ctr) {
+    if (leaf >= 0 && inside_leaf(s, leaf, xw, leaf_nudge(xw))) return leaf;
+    bool scanned = false;
+    const int L = find_leaf(s, xw, &scanned);
+    ctr.scans += scanned;
+    if (L >= 0 && L != leaf) {
+#pragma unroll
+      for (int d = 0; d < 3; d++) idxc[d] = fastm::rcp(ldg(s.dxc + 3 * L + d));  // feeds only the step cap
+    }
+    leaf = L;
+    return L;
+  }
+
+  // One pass of the march loop; false once the ray has ended.
+  //
+  // The reference processes each point's plasma sample one pass late (core/render/pixel.hpp:179-211), after the
+  // next point's leaf lookup, whose leaf then seeds the sampler's cache check.  FP64 keeps that order, so that it
+  // follows the reference bit for bit.  The FP32 paths process each sample at its own point, before the step, seeded
+  // by its own leaf (found for the step-size cap anyway): the samples, their order and their segment lengths are the
+  // same (points 1.. of the live path inside rt_outer, each with the length of the step that led to it), no copy of
+  // the previous point's state is carried (fewer registers), and the leaf found differs only for points within the
+  // sampler's 1e-9 nudge of a block face, which FP32 positions do not resolve anyway.
   PHX_HD bool advance(const SnapView<R, PT>& s, const RenderConsts<R>& rc, RayCounters& ctr) {
     R cx[4], ck[4], cF[4];
 #pragma unroll
@@ -134,51 +159,49 @@ struct Ray {
     }
     const R r = exp_t(cx[1]);
     const bool alive = r < rc.r_out && r > rc.cut_in && steps < rc.max_steps && !terminate;
-    // The pending sample's plasma stage only runs inside rt_outer (the reference samples the fluid further out too,
-    // but always discards it there: derive_fluid and process_sample both require r < rt_outer, and the sampler cache
-    // the lookup seeds is local to that sample), so its cache seed is only needed then.
-    const bool pend_plasma = pvalid && pr < rc.rt_outer;
-    const bool need_leaf = pend_plasma && alive;
-    const bool need_dxc = alive && r < rc.rt_outer;
-    int L = -1, right = -1;
-    if (need_leaf || need_dxc) {
-      // the step-size cap and the sample's cache seed: FP32 in every FP32 mode (mixed re-checks the seed in FP64)
-      R xw[4] = {cx[0], cx[1], cx[2], cx[3]};
-      wrap_coords(xw);
-      // a ray stays tens of steps in one leaf: test the last one before the map (the leaves tile the domain, so a
-      // point inside it has no other leaf)
-      if (leaf >= 0 && inside_leaf(s, leaf, xw, leaf_nudge(xw))) {
-        L = leaf;
-      } else {
-        bool scanned = false;
-        L = find_leaf(s, xw, &scanned);
-        ctr.scans += scanned;
-        if (L >= 0 && L != leaf) {
-#pragma unroll
-          for (int d = 0; d < 3; d++) idxc[d] = R(1) / ldg(s.dxc + 3 * L + d);
-        }
-        leaf = L;
+    // beyond rt_outer the reference keeps no sample (derive_fluid and process_sample both require r < rt_outer) and
+    // caps no step by the grid
+    const bool inner = alive && r < rc.rt_outer;
+    int L = -1;
+    if constexpr (kLate) {
+      const bool pend_plasma = pvalid && pr < rc.rt_outer;
+      const bool need_leaf = pend_plasma && alive;
+      int right = -1;
+      if (need_leaf || inner) {
+        R xw[4] = {cx[0], cx[1], cx[2], cx[3]};
+        wrap_coords(xw);
+        L = lookup(s, xw, ctr);
+        if (need_leaf) right = (r < R(1) || outside_domain(s, xw)) ? -1 : L;  // wrapping keeps x1: exp(xw[1]) = r
       }
-      if (need_leaf) right = (r < R(1) || outside_domain(s, xw)) ? -1 : L;  // wrapping keeps x1: exp(xw[1]) = r
-    }
-    if (pend_plasma) process_sample(s, rc, right, ctr);
+      if (pend_plasma) process_sample(s, rc, px, pk, pF, pr, pdl, right, ctr);
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-      px[i] = cx[i];
-      pk[i] = ck[i];
-      pF[i] = cF[i];
-      if constexpr (kMixed) pxd[i] = (double)geo.hi[i] + (double)geo.lo[i];
+      for (int i = 0; i < 4; i++) {
+        px[i] = cx[i];
+        pk[i] = ck[i];
+        pF[i] = cF[i];
+      }
+      pr = r;
+      pdl = dl_prev;
+      pvalid = steps >= 1;
+      if (!alive) return false;
+    } else {
+      if (!alive) return false;
+      if (inner) {
+        R xw[4] = {cx[0], cx[1], cx[2], cx[3]};
+        wrap_coords(xw);
+        L = lookup(s, xw, ctr);
+        if (steps >= 1) {
+          const int right = (r < R(1) || outside_domain(s, xw)) ? -1 : L;  // wrapping keeps x1: exp(xw[1]) = r
+          process_sample(s, rc, cx, ck, cF, r, dl_prev, right, ctr);
+        }
+      }
     }
-    pr = r;
-    pdl = dl_prev;
-    pvalid = steps >= 1;
-    if (!alive) return false;
 
     if (thdot_prev * ck[2] < R(0) && steps > 2) turns++;
     thdot_prev = ck[2];
     if ((bsign < 0 && turns > rc.max_order) || (bsign > 0 && turns > rc.max_order + 1)) terminate = true;
 
-    const bool cap = need_dxc && L >= 0;
+    const bool cap = inner && L >= 0;
     const R x2 = pole_x2<R, kComp>(geo);
     R dl;
     if constexpr (sizeof(R) == 4) {
@@ -207,16 +230,17 @@ struct Ray {
     return true;
   }
 
-  // The plasma stage of the pending sample (the reference's process_sample, core/render/pixel.hpp:52-123).
-  PHX_HD void process_sample(const SnapView<R, PT>& s, const RenderConsts<R>& rc, int right, RayCounters& ctr) {
-    R k[4] = {pk[0], pk[1], pk[2], pk[3]};
-    const R r = pr;
+  // The plasma stage of the sample at point (x0, k0, F0) of radius r, reached by a step of length hl (the reference's
+  // process_sample, core/render/pixel.hpp:52-123).
+  PHX_HD void process_sample(const SnapView<R, PT>& s, const RenderConsts<R>& rc, const R x0[4], const R k0[4],
+                             const R F0[4], R r, R hl, int right, RayCounters& ctr) {
+    R k[4] = {k0[0], k0[1], k0[2], k0[3]};
     {
-      const KerrPt<R> p0 = kerr_point_r(s.a, s.hs, r, px[2]);
+      const KerrPt<R> p0 = kerr_point_r(s.a, s.hs, r, x0[2]);
       const Cov<R> g0 = cov_metric(p0, s.a);
       if (fabs_t(dot(g0, k, k)) > R(1e-6) && r > R(2)) {
         if constexpr (kMixed) {
-          const KerrPt<double> pd = kerr_point((double)s.a, (double)s.hs, (double)px[1], (double)px[2]);
+          const KerrPt<double> pd = kerr_point((double)s.a, (double)s.hs, (double)x0[1], (double)x0[2]);
           const Cov<double> gd = cov_metric(pd, (double)s.a);
           double kd[4] = {k[0], k[1], k[2], k[3]};
           normalize_null(gd, kd);
@@ -227,11 +251,14 @@ struct Ray {
       }
     }
     // sampler (sampler.hpp:387-427): wrap, domain, cached leaf or a fresh lookup of the re-wrapped point
-    R x[4] = {px[0], px[1], px[2], px[3]};
+    R x[4] = {x0[0], x0[1], x0[2], x0[3]};
     int ig = right;
     R q[kNPrim];
     if constexpr (kMixed) {
-      double xd[4] = {pxd[0], pxd[1], pxd[2], pxd[3]};
+      // the compensated position of this point (mixed processes samples before the step: the state is this point's)
+      double xd[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) xd[i] = (double)geo.hi[i] + (double)geo.lo[i];
       const SnapView<double, PT> sd = s.fp64_view();
       wrap_coords(xd);
       if (exp_t(xd[1]) < 1.0) return;
@@ -292,7 +319,7 @@ struct Ray {
     // polarization axes of the plasma frame with B as reference direction; EVPA rotation from the transported F1
     R perp[4], para[4], pFd[4];
     observer_axes_lowered(sqrt_neg_g(p), k, fl.U, fl.B, kd, Ud, Bd, -kU, kB, UB, BB, perp, para);
-    symv(g, pF, pFd);
+    symv(g, F0, pFd);
     const R C = dot4(pFd, perp), S = dot4(pFd, para);
     const R inn = fastm::rcp(C * C + S * S);
     const R c2 = (C * C - S * S) * inn, s2 = R(2) * C * S * inn;
@@ -305,7 +332,7 @@ struct Ray {
       const Coeffs<R> cf = synchro_coeffs(ss, nu, rc.jscale[f]);
       R K[4][4], jv[4], E[4][4], Sg[4];
       build_K(cf, c2, s2, K, jv);
-      const R h = pdl * rc.hconst[f];
+      const R h = hl * rc.hconst[f];
       bool fp64 = false;
       if constexpr (kMixed) {
         const R kmax = fmax_t(fmax_t(fabs_t(cf.aI), fabs_t(cf.rV)), fabs_t(cf.rQ));
