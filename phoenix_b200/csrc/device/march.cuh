@@ -54,7 +54,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
   const unsigned lane = threadIdx.x & 31u;
   RayT ray;
   RayCounters ctr{};
-  unsigned long long steps = 0, nplasma = 0, bad = 0, rays = 0;
+  // per-lane sums in 32 bits (a launch gives a lane at most ~2^31 / lanes rays of <= max_steps steps: far below 2^32)
+  unsigned steps = 0, nplasma = 0, bad = 0, rays = 0;
   bool live = false, drained = false;
   for (;;) {
     if (!drained) {
@@ -97,18 +98,16 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
       }
     }
   }
-  steps = warp_sum_u64(steps);
-  nplasma = warp_sum_u64(nplasma);
-  bad = warp_sum_u64(bad);
-  rays = warp_sum_u64(rays);
+  const unsigned long long wsteps = warp_sum_u64(steps), wnplasma = warp_sum_u64(nplasma), wbad = warp_sum_u64(bad),
+                           wrays = warp_sum_u64(rays);
   const unsigned long long scans = warp_sum_u64(ctr.scans);
   const unsigned long long f64s = warp_sum_u64(ctr.fp64_steps);
   const unsigned long long f64o = warp_sum_u64(ctr.fp64_ops);
   if (lane == 0) {
-    atomicAdd(&A.counters[kCtrSteps], steps);
-    atomicAdd(&A.counters[kCtrPlasma], nplasma);
-    atomicAdd(&A.counters[kCtrBad], bad);
-    atomicAdd(&A.counters[kCtrRays], rays);
+    atomicAdd(&A.counters[kCtrSteps], wsteps);
+    atomicAdd(&A.counters[kCtrPlasma], wnplasma);
+    atomicAdd(&A.counters[kCtrBad], wbad);
+    atomicAdd(&A.counters[kCtrRays], wrays);
     if (scans) atomicAdd(&A.counters[kCtrScans], scans);
     if (f64s) atomicAdd(&A.counters[kCtrFp64Steps], f64s);
     if (f64o) atomicAdd(&A.counters[kCtrFp64Ops], f64o);
