@@ -90,69 +90,110 @@ PHX_HD bool all_finite(const R E[4][4], const R S[4]) {
   return s == R(0);  // any inf or NaN makes the sum NaN
 }
 
-// Per-ray, per-frequency accumulator.  kKahan: compensated summation of the Stokes vector.
-template <class R, bool kKahan>
-struct StokesAcc {
-  R X[4][4];  // D = A - I while `dev`, else A
-  R S[4];
-  R Sc[4];
-  R tau, tauF;
-  bool dev;
+// Per-ray, per-frequency accumulator record, as words of precision R:
+//   X[4][4]  D = A - I while in deviation form, else A;   S[4] Stokes sums;   Sc[4] their Kahan compensation (kKahan);
+//   tau, tauF;   dev (1: X holds D, 0: X holds A).
+template <bool kKahan>
+struct AccWords {
+  static constexpr int kX = 0, kS = 16, kSc = 20, kTau = kKahan ? 24 : 20, kTauF = kTau + 1, kDev = kTau + 2,
+                       kN = kTau + 3;
+};
 
-  PHX_HD void reset() {
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-#pragma unroll
-      for (int k = 0; k < 4; k++) X[i][k] = R(0);
-      S[i] = R(0);
-      Sc[i] = R(0);
-    }
-    tau = tauF = R(0);
-    dev = true;
-  }
+// Records in the thread's registers (FP64 and the 32-slot kernels).
+template <class R, bool kKahan, int NF>
+struct AccRegs {
+  static constexpr size_t kSmemPerThread = 0;
+  R w[NF][AccWords<kKahan>::kN];
+  PHX_HD R& at(int f, int e) { return w[f][e]; }
+};
 
-  PHX_HD void add(const R E[4][4], const R Sg[4]) {
-    // Stokes: S += A S_seg with the accumulated operator before this segment
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-      R t = dev ? Sg[i] : R(0);
-#pragma unroll
-      for (int k = 0; k < 4; k++) t += X[i][k] * Sg[k];
-      if (kKahan) {
-        const R y = t - Sc[i];
-        const R s = S[i] + y;
-        Sc[i] = (s - S[i]) - y;
-        S[i] = s;
-      } else {
-        S[i] += t;
-      }
-    }
-    // transmission: X <- X + X E (+ E in deviation form)
-    R Y[4][4];
-#pragma unroll
-    for (int i = 0; i < 4; i++)
-#pragma unroll
-      for (int k = 0; k < 4; k++) {
-        R t = dev ? E[i][k] : R(0);
-#pragma unroll
-        for (int m = 0; m < 4; m++) t += X[i][m] * E[m][k];
-        Y[i][k] = t;
-      }
-#pragma unroll
-    for (int i = 0; i < 4; i++)
-#pragma unroll
-      for (int k = 0; k < 4; k++) X[i][k] += Y[i][k];
-    if (dev) {
-      R m = R(0);
-#pragma unroll
-      for (int i = 0; i < 4; i++) m = fmax_t(m, fabs_t(X[i][i]));
-      if (m > R(0.5)) {
-#pragma unroll
-        for (int i = 0; i < 4; i++) X[i][i] += R(1);
-        dev = false;
-      }
-    }
+#if defined(__CUDACC__)
+extern __shared__ __align__(16) unsigned char phx_dyn_smem[];
+#endif
+
+// Records in the block's dynamic shared memory: word e of slot f of a thread at [(f * kN + e) * blockDim.x + tid],
+// so the 32 lanes of a warp touch 32 consecutive words (no bank conflicts).  Keeping the 4x4 operator out of the
+// registers shortens the live state the geodesic step carries by a record per slot (23 words in FP32).
+template <class R, bool kKahan, int NF>
+struct AccShared {
+  static constexpr size_t kSmemPerThread = sizeof(R) * NF * AccWords<kKahan>::kN;
+  PHX_HD R& at(int f, int e) {
+#if defined(__CUDA_ARCH__)
+    return reinterpret_cast<R*>(phx_dyn_smem)[(f * AccWords<kKahan>::kN + e) * blockDim.x + threadIdx.x];
+#else
+    static R unused;  // device-only storage
+    return unused;
+#endif
   }
 };
+
+template <class R, bool kKahan, class St>
+PHX_HD void acc_reset(St& st, int f) {
+  using W = AccWords<kKahan>;
+#pragma unroll
+  for (int e = 0; e < W::kN; e++) st.at(f, e) = R(0);
+  st.at(f, W::kDev) = R(1);
+}
+
+// Appends one segment (E = A_seg - I, Sg = S_seg) and its optical depths to slot f:
+//   S += A Sg with the accumulated operator before this segment (Kahan-compensated when kKahan);
+//   X <- X + X E (+ E in deviation form), switching to the plain form once |D_ii| > 1/2.
+template <class R, bool kKahan, class St>
+PHX_HD void acc_add(St& st, int f, const R E[4][4], const R Sg[4], R dtau, R dtauF) {
+  using W = AccWords<kKahan>;
+  R X[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int k = 0; k < 4; k++) X[i][k] = st.at(f, W::kX + 4 * i + k);
+  bool dev = st.at(f, W::kDev) != R(0);
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    R t = dev ? Sg[i] : R(0);
+#pragma unroll
+    for (int k = 0; k < 4; k++) t += X[i][k] * Sg[k];
+    const R S = st.at(f, W::kS + i);
+    if constexpr (kKahan) {
+      const R c = st.at(f, W::kSc + i);
+      const R y = t - c;
+      const R s = S + y;
+      st.at(f, W::kSc + i) = (s - S) - y;
+      st.at(f, W::kS + i) = s;
+    } else {
+      st.at(f, W::kS + i) = S + t;
+    }
+  }
+  R Y[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      R t = dev ? E[i][k] : R(0);
+#pragma unroll
+      for (int m = 0; m < 4; m++) t += X[i][m] * E[m][k];
+      Y[i][k] = t;
+    }
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int k = 0; k < 4; k++) X[i][k] += Y[i][k];
+  if (dev) {
+    R m = R(0);
+#pragma unroll
+    for (int i = 0; i < 4; i++) m = fmax_t(m, fabs_t(X[i][i]));
+    if (m > R(0.5)) {
+#pragma unroll
+      for (int i = 0; i < 4; i++) X[i][i] += R(1);
+      dev = false;
+      st.at(f, W::kDev) = R(0);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int k = 0; k < 4; k++) st.at(f, W::kX + 4 * i + k) = X[i][k];
+  st.at(f, W::kTau) += dtau;
+  st.at(f, W::kTauF) += dtauF;
+}
 
 }  // namespace phx

@@ -11,11 +11,17 @@ template <Mode M, class PT, int NF, int kMinBlocks>
 cudaError_t launch_mb(const MarchArgs<typename Policy<M>::R, PT>& args, int sms, cudaStream_t stream,
                       LaunchShape* shape) {
   auto kern = k_march<M, PT, NF, kBlock, kMinBlocks>;
+  // the rays' transfer records (shared-memory kernels; 0 otherwise)
+  const size_t smem = Ray<M, PT, NF>::kSmemPerThread * kBlock;
   cudaFuncAttributes fa;
   cudaError_t e = cudaFuncGetAttributes(&fa, kern);
   if (e != cudaSuccess) return e;
+  if (smem > 48 * 1024) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
   int bpsm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, kern, kBlock, 0);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, kern, kBlock, smem);
   if (e != cudaSuccess) return e;
   if (bpsm < 1) bpsm = 1;
   long long grid = (long long)bpsm * sms;
@@ -28,7 +34,7 @@ cudaError_t launch_mb(const MarchArgs<typename Policy<M>::R, PT>& args, int sms,
   shape->local_bytes = (int)fa.localSizeBytes;
   shape->blocks_per_sm = bpsm;
   if (args.njobs <= 0) return cudaSuccess;
-  kern<<<(unsigned)grid, kBlock, 0, stream>>>(args);
+  kern<<<(unsigned)grid, kBlock, smem, stream>>>(args);
   return cudaGetLastError();
 }
 

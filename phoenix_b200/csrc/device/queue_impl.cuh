@@ -13,11 +13,17 @@ template <Mode M, class PT, int NF, int kMinBlocks>
 cudaError_t launch_queue_mb(const QueueArgs<typename Policy<M>::R, PT>& args, int sms, int period, long long max_rays,
                             cudaStream_t stream, LaunchShape* shape) {
   auto kern = k_queue<M, PT, NF, kQueueBlock, kMinBlocks>;
+  // the rays' transfer records (shared-memory kernels; 0 otherwise)
+  const size_t smem = Ray<M, PT, NF>::kSmemPerThread * kQueueBlock;
   cudaFuncAttributes fa;
   cudaError_t e = cudaFuncGetAttributes(&fa, kern);
   if (e != cudaSuccess) return e;
+  if (smem > 48 * 1024) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
   int bpsm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, kern, kQueueBlock, 0);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, kern, kQueueBlock, smem);
   if (e != cudaSuccess) return e;
   if (bpsm < 1) bpsm = 1;
   long long grid = (long long)bpsm * sms;
@@ -30,7 +36,7 @@ cudaError_t launch_queue_mb(const QueueArgs<typename Policy<M>::R, PT>& args, in
   shape->blocks_per_sm = bpsm;
   QueueArgs<typename Policy<M>::R, PT> a = args;
   a.period = period > 0 ? period : 32;
-  kern<<<(unsigned)grid, kQueueBlock, 0, stream>>>(a);
+  kern<<<(unsigned)grid, kQueueBlock, smem, stream>>>(a);
   return cudaGetLastError();
 }
 
