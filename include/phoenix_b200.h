@@ -97,10 +97,11 @@ typedef struct {
   int32_t precision;   /* PHX_PREC_* */
   double r_fp64;       /* mixed: FP64 RK4 inside r < r_fp64 * r_horizon (<= 0: default 3, the photon-orbit region) */
   double tau_fp64;     /* mixed: FP64 segment operator where h max|K| exceeds this (<= 0: default 0.1) */
-  int32_t block;       /* threads per block, 0 = default */
-  int32_t period;      /* march passes between lane refills, 0 = default (32) */
-  int32_t blocks_per_sm; /* register-cap variant: resident 128-thread blocks per SM the kernel is compiled for
-                            (1: up to 255 registers, 3: 168, 4: 128); 0 = default (3; mixed: 1) */
+  int32_t block;       /* unused (the block shape follows blocks_per_sm; PhxRenderInfo.block reports it) */
+  int32_t period;      /* march passes between lane refills, 0 = default (64) */
+  int32_t blocks_per_sm; /* register-cap variant, as resident warps per SM / 4 (1: up to 255 registers in 128-thread
+                            blocks; 3: 168 registers, 4: 128, as one 384 / 512-thread block per SM when the job list
+                            fills every SM, else as 128-thread blocks); 0 = default (FP32 4; mixed, FP64 1) */
 } PhxRenderParams;
 
 /* What a render reports (a superset of the reference's device::Info, src/device/kernel.cuh:23-30). */
@@ -207,8 +208,8 @@ typedef struct {
 
 typedef struct {
   int32_t tile_rays;       /* rays per queue tile, 0 = 32 */
-  int32_t blocks_per_sm;   /* register-cap variant (FP32: 1, 3, 4), 0 = default 3 or autotuned */
-  int32_t period;          /* march passes between lane refills, 0 = default 32 or autotuned */
+  int32_t blocks_per_sm;   /* register-cap variant (FP32: 1, 3, 4; mixed 1, 3), 0 = default (FP32 4, else 1) or autotuned */
+  int32_t period;          /* march passes between lane refills, 0 = default 64 or autotuned */
   int32_t autotune;        /* nonzero: time every (blocks_per_sm, period) candidate on a sample of the batch's tiles
                               at creation and keep the fastest */
   int32_t sample_stride;   /* autotune sample: every n-th tile, 0 = 16 */
@@ -267,8 +268,8 @@ typedef struct {
   int32_t precision;      /* PHX_PREC_*, shared by every request */
   int32_t max_freqs;      /* frequency slots per request (1 or 4; FP32 also up to 32), default 4 */
   int32_t tile_rays;      /* rays per queue tile, default 32 */
-  int32_t period;         /* march passes between lane refills, default 32 */
-  int32_t blocks_per_sm;  /* register-cap variant, default 3 */
+  int32_t period;         /* march passes between lane refills, default 64 */
+  int32_t blocks_per_sm;  /* register-cap variant, 0 = default (FP32 4, else 1) */
   int32_t max_items;      /* requests per run of the kernel before the queue is recycled, default 4096 */
   int64_t max_tiles;      /* tiles per run of the kernel, a power of two, default 2^22 */
   int32_t idle_ns;        /* sleep of an idle warp between polls of the queue, default 2000 */

@@ -38,7 +38,7 @@ cudaError_t launch_mode(PhxSnapshot* s, const PhxRenderParams& p, const typename
   A.out = reinterpret_cast<double*>(d_res);
   A.pixstats = d_pixstats;
   A.counters = reinterpret_cast<unsigned long long*>(d_counters);
-  A.period = p.period > 0 ? p.period : 32;  // passes between lane refills (measured best on B200)
+  A.period = p.period > 0 ? p.period : phx::kDefaultPeriod;  // passes between lane refills (measured best on B200)
   return phx::launch_march<M, PT>(A, s->sms, p.blocks_per_sm, st, shape);
 }
 

@@ -114,6 +114,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
   }
 }
 
+// Default march passes between lane refills (measured best on B200 for the single-image and queue kernels).
+constexpr int kDefaultPeriod = 64;
+
 // Launch entry per (mode, prim type): picks the frequency-slot instantiation and the launch shape.
 struct LaunchShape {
   int block, grid, regs, local_bytes, blocks_per_sm;

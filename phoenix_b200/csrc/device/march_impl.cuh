@@ -5,9 +5,14 @@
 
 namespace phx {
 
-constexpr int kBlock = 128;
-
-template <Mode M, class PT, int NF, int kMinBlocks>
+// Launch shapes.  `blocks_per_sm` names a register-cap variant by its resident warps per SM / 4:
+//   1: 128-thread blocks, up to 255 registers (the compiler takes 192 in FP32: 2 blocks, 8 warps per SM);
+//   3: 168 registers, 12 warps per SM;   4: 128 registers, 16 warps per SM.
+// Variants 3 and 4 run as ONE block of 384 / 512 threads per SM when the job list gives every SM such a block, and as
+// 3 / 4 blocks of 128 threads otherwise (small images then still spread over all SMs).  On B200 the whole-SM block
+// measured faster than the same warps in 128-thread blocks: FP32, 3 x 512^2 bench images, 16 warps 326 ms as one
+// block vs 379 ms as four; 12 warps 336 vs 349 ms.
+template <Mode M, class PT, int NF, int kBlock, int kMinBlocks>
 cudaError_t launch_mb(const MarchArgs<typename Policy<M>::R, PT>& args, int sms, cudaStream_t stream,
                       LaunchShape* shape) {
   auto kern = k_march<M, PT, NF, kBlock, kMinBlocks>;
@@ -38,28 +43,34 @@ cudaError_t launch_mb(const MarchArgs<typename Policy<M>::R, PT>& args, int sms,
   return cudaGetLastError();
 }
 
-// Register-cap variants: `blocks_per_sm` picks the instantiation compiled for that many resident 128-thread blocks
-// per SM (__launch_bounds__ min blocks: 1 -> up to 255 registers, 3 -> 168, 4 -> 128; 0 = default).  FP64 and the 32-slot
-// variants are compiled uncapped only.
+// Default variant per mode (measured on B200): FP32 4 (128 registers, 16 warps); mixed 1 (it spills at 168).
+template <Mode M>
+constexpr int default_blocks_per_sm() {
+  return M == Mode::kFP32 ? 4 : 1;
+}
+
+// The variant for `blocks_per_sm` (0 = the mode's default).  FP64 and the 32-slot kernels are compiled uncapped only;
+// mixed offers 1 and 3.
 template <Mode M, class PT, int NF>
 cudaError_t launch_nf(const MarchArgs<typename Policy<M>::R, PT>& args, int sms, int blocks_per_sm,
                       cudaStream_t stream, LaunchShape* shape) {
   if constexpr (M == Mode::kFP64 || NF > 4) {
     (void)blocks_per_sm;
-    return launch_mb<M, PT, NF, 1>(args, sms, stream, shape);
+    return launch_mb<M, PT, NF, 128, 1>(args, sms, stream, shape);
   } else {
-    switch (blocks_per_sm) {
-      case 1:
-      case 2:
-        return launch_mb<M, PT, NF, 1>(args, sms, stream, shape);
-      case 3:
-        return launch_mb<M, PT, NF, 3>(args, sms, stream, shape);
-      case 4:
-        return launch_mb<M, PT, NF, 4>(args, sms, stream, shape);
-      default:  // measured on B200: FP32 3 resident blocks (168 registers); mixed uncapped (it spills at 168)
-        if constexpr (M == Mode::kMixed) return launch_mb<M, PT, NF, 1>(args, sms, stream, shape);
-        else return launch_mb<M, PT, NF, 3>(args, sms, stream, shape);
+    const int bps = blocks_per_sm > 0 ? blocks_per_sm : default_blocks_per_sm<M>();
+    const bool whole = args.njobs >= (long long)sms * 128 * bps;  // a whole-SM block for every SM
+    if (bps == 3) {
+      return whole ? launch_mb<M, PT, NF, 384, 1>(args, sms, stream, shape)
+                   : launch_mb<M, PT, NF, 128, 3>(args, sms, stream, shape);
     }
+    if constexpr (M == Mode::kFP32) {
+      if (bps == 4) {
+        return whole ? launch_mb<M, PT, NF, 512, 1>(args, sms, stream, shape)
+                     : launch_mb<M, PT, NF, 128, 4>(args, sms, stream, shape);
+      }
+    }
+    return launch_mb<M, PT, NF, 128, 1>(args, sms, stream, shape);
   }
 }
 

@@ -191,9 +191,15 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
 
 // Launch configuration of the queue kernel (the autotuner's search space).
 struct QueueShape {
-  int blocks_per_sm;  // register-cap variant: 1, 3 or 4 (FP32); mixed 3; FP64 1
+  int blocks_per_sm;  // register-cap variant: 1, 3 or 4 (FP32); mixed 1 or 3; FP64 1; 0 = the mode's default
   int period;
 };
+
+// Default register-cap variant (measured on B200): FP32 128 registers (16 warps per SM), mixed and FP64 uncapped.
+template <Mode M>
+constexpr int default_queue_blocks_per_sm() {
+  return M == Mode::kFP32 ? 4 : 1;
+}
 
 // Launches the queue kernel for `nf_slots` frequency slots (1, 4 or 32) on a persistent grid (resident blocks x SMs),
 // capped at the blocks `max_rays` rays can fill when max_rays > 0.

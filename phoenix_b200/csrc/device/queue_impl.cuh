@@ -7,9 +7,7 @@
 
 namespace phx {
 
-constexpr int kQueueBlock = 128;
-
-template <Mode M, class PT, int NF, int kMinBlocks>
+template <Mode M, class PT, int NF, int kQueueBlock, int kMinBlocks>
 cudaError_t launch_queue_mb(const QueueArgs<typename Policy<M>::R, PT>& args, int sms, int period, long long max_rays,
                             cudaStream_t stream, LaunchShape* shape) {
   auto kern = k_queue<M, PT, NF, kQueueBlock, kMinBlocks>;
@@ -40,26 +38,29 @@ cudaError_t launch_queue_mb(const QueueArgs<typename Policy<M>::R, PT>& args, in
   return cudaGetLastError();
 }
 
-// Register-cap variants as for the single-image kernel: FP32 is compiled for 1, 3 and 4 resident 128-thread blocks
-// per SM with one and four frequency slots; mixed for 1 and 3; FP64 and 32 slots uncapped.
+// Register-cap variants and block shapes as for the single-image kernel (march_impl.cuh): `blocks_per_sm` 1 -> 128-thread
+// blocks at up to 255 registers; 3 / 4 -> 168 / 128 registers as one 384 / 512-thread block per SM, or as 128-thread
+// blocks when the work (max_rays; <= 0: unbounded, a serving loop) cannot give every SM a whole block.  FP32 offers
+// 1, 3, 4; mixed 1 and 3; FP64 and 32 slots are uncapped only.
 template <Mode M, class PT, int NF>
 cudaError_t launch_queue_nf(const QueueArgs<typename Policy<M>::R, PT>& args, int sms, QueueShape q,
                             long long max_rays, cudaStream_t stream, LaunchShape* shape) {
   if constexpr (M == Mode::kFP64 || NF > 4) {
-    return launch_queue_mb<M, PT, NF, 1>(args, sms, q.period, max_rays, stream, shape);
-  } else if constexpr (M == Mode::kMixed) {
-    if (q.blocks_per_sm == 3) return launch_queue_mb<M, PT, NF, 3>(args, sms, q.period, max_rays, stream, shape);
-    return launch_queue_mb<M, PT, NF, 1>(args, sms, q.period, max_rays, stream, shape);
+    return launch_queue_mb<M, PT, NF, 128, 1>(args, sms, q.period, max_rays, stream, shape);
   } else {
-    switch (q.blocks_per_sm) {
-      case 1:
-      case 2:
-        return launch_queue_mb<M, PT, NF, 1>(args, sms, q.period, max_rays, stream, shape);
-      case 4:
-        return launch_queue_mb<M, PT, NF, 4>(args, sms, q.period, max_rays, stream, shape);
-      default:
-        return launch_queue_mb<M, PT, NF, 3>(args, sms, q.period, max_rays, stream, shape);
+    const int bps = q.blocks_per_sm > 0 ? q.blocks_per_sm : default_queue_blocks_per_sm<M>();
+    const bool whole = max_rays <= 0 || max_rays >= (long long)sms * 128 * bps;
+    if (bps == 3) {
+      return whole ? launch_queue_mb<M, PT, NF, 384, 1>(args, sms, q.period, max_rays, stream, shape)
+                   : launch_queue_mb<M, PT, NF, 128, 3>(args, sms, q.period, max_rays, stream, shape);
     }
+    if constexpr (M == Mode::kFP32) {
+      if (bps == 4) {
+        return whole ? launch_queue_mb<M, PT, NF, 512, 1>(args, sms, q.period, max_rays, stream, shape)
+                     : launch_queue_mb<M, PT, NF, 128, 4>(args, sms, q.period, max_rays, stream, shape);
+      }
+    }
+    return launch_queue_mb<M, PT, NF, 128, 1>(args, sms, q.period, max_rays, stream, shape);
   }
 }
 

@@ -532,7 +532,7 @@ PhxServer* create_server(PhxSnapshot* const* snaps, int32_t nsnaps, const PhxSer
   if ((o.max_tiles & (o.max_tiles - 1)) != 0) throw std::invalid_argument("max_tiles must be a power of two");
   if (o.max_freqs <= 0) o.max_freqs = 4;
   if (o.max_freqs > 4 && o.precision != PHX_PREC_FP32) throw std::invalid_argument("more than 4 frequencies: FP32 only");
-  if (o.period <= 0) o.period = 32;
+  if (o.period <= 0) o.period = phx::kDefaultPeriod;
   if (o.idle_ns <= 0) o.idle_ns = 2000;
   if (o.idle_limit <= 0) o.idle_limit = 5000000;
   if (o.linger_ms < 0) o.linger_ms = 0;
@@ -605,8 +605,8 @@ void phx_default_server_options(PhxServerOptions* o) {
   o->precision = PHX_PREC_FP32;
   o->max_freqs = 4;
   o->tile_rays = 32;
-  o->period = 32;
-  o->blocks_per_sm = 3;
+  o->period = phx::kDefaultPeriod;
+  o->blocks_per_sm = 0;
   o->max_items = 4096;
   o->max_tiles = 1 << 22;
   o->idle_ns = 2000;

@@ -134,6 +134,33 @@ def test_results_independent_of_scheduling(gpu_snapshots, bps):
     assert l1 <= 1e-5, l1
 
 
+@pytest.mark.parametrize("bps", [3, 4])
+def test_whole_sm_blocks(gpu_snapshots, bps):
+    """Register-cap variants 3 and 4 run as one 384 / 512-thread block per SM once the job list gives every SM such a
+    block (a 320^2 image: 102,400 rays >= 148 SMs x 512).  That shape is bit-identical across refill periods, agrees
+    with the 128-thread shape of the same cap (a small job subset; separate compilations round differently) within
+    1e-4 L1, and matches the FP64 render to the FP32 flux bar."""
+    kw = case_params("cfg1")
+    kw.update(img=320, fov_x=2 * kw["fov_x"], fov_y=2 * kw["fov_y"])
+    snap = gpu_snapshots["cfg1"]
+    base, info = snap.render(P.make_params(precision="fp32", blocks_per_sm=bps, period=64, **kw))
+    assert info["block"] == 128 * bps and info["blocks"] == info["sms"], info
+    other, _ = snap.render(P.make_params(precision="fp32", blocks_per_sm=bps, period=4, **kw))
+    assert np.array_equal(base, other)
+    # 2,048 jobs: too few for whole-SM blocks, so the same pixels run on the 128-thread shape
+    jobs = P.schedule_morton(320, 320)[::50].copy()
+    small, sinfo = snap.render(P.make_params(precision="fp32", blocks_per_sm=bps, **kw), jobs=jobs)
+    assert sinfo["block"] == 128, sinfo
+    sel = np.sort(jobs)
+    a, b = small.reshape(-1, 6)[sel], base.reshape(-1, 6)[sel]
+    assert np.abs(a[:, :4] - b[:, :4]).sum() <= 1e-4 * np.abs(b[:, :4]).sum()
+    p64 = P.make_params(precision="fp64", **kw)
+    ref, _ = snap.render(p64)
+    f, g = P.flux(base, p64), P.flux(ref, p64)
+    assert np.abs(f[:, 0] - g[:, 0]).max() <= 1e-4 * np.abs(g[:, 0]).max()
+    assert np.abs(f[:, 1:] - g[:, 1:]).max() <= 1e-3 * np.abs(g[:, 0]).max()
+
+
 def test_invalid_arguments_are_reported(gpu_snapshots):
     p = P.make_params(img=0)
     with pytest.raises(P.PhxError) as e:
