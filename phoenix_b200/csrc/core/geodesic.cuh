@@ -1,6 +1,7 @@
 // Geodesic state and RK4 integrator of the raymarch.
 //
-// The state is (x^mu, k^mu, F^mu): position, wave vector and the parallel-transported camera polarization vector.
+// The state is (x^mu, k^mu, F^mu): position, wave vector and the parallel-transported camera polarization vector
+// (NS = 12), or (x^mu, k^mu) alone (NS = 8) when the polarization comes from the Walker-Penrose constant (kerr.cuh).
 // At FP32 it is carried as hi + lo float pairs updated by compensated (TwoSum) addition, and a ray in the southern
 // hemisphere is integrated in the mirror coordinate pi - x2 so that x2 keeps its precision next to the south pole
 // (the same device the reference's FP32 build uses, core/geometry/geodesic.hpp:200-256).  At FP64 the lo half is
@@ -25,32 +26,33 @@ PHX_HD void comp_add(R& hi, R& lo, R d) {
   hi = s2;
 }
 
-template <class R>
+template <class R, int NS = 12>
 struct GeoState {
-  R hi[12];  // x[0..3], k[4..7], F[8..11]
-  R lo[12];  // compensation (FP32 only)
+  static constexpr int kN = NS;
+  R hi[NS];  // x[0..3], k[4..7], F[8..11] (NS = 12)
+  R lo[NS];  // compensation (FP32 only)
 };
 
-// Initial state from the FP64 camera photon and polarization vector.
-template <class R, bool kComp>
-PHX_HD void geo_init(GeoState<R>& g, const double ph[8], const double F[4]) {
-  for (int i = 0; i < 8; i++) g.hi[i] = R(ph[i]);
-  for (int i = 0; i < 4; i++) g.hi[8 + i] = R(F[i]);
-  for (int i = 0; i < 12; i++) g.lo[i] = R(0);
-  if (kComp) {
-    for (int i = 0; i < 8; i++) g.lo[i] = R(ph[i] - (double)g.hi[i]);
-    for (int i = 0; i < 4; i++) g.lo[8 + i] = R(F[i] - (double)g.hi[8 + i]);
+// Initial state from the FP64 camera photon and polarization vector (F unused when NS = 8).
+template <class R, bool kComp, int NS>
+PHX_HD void geo_init(GeoState<R, NS>& g, const double ph[8], const double F[4]) {
+  double v[12];
+  for (int i = 0; i < 8; i++) v[i] = ph[i];
+  for (int i = 0; i < 4; i++) v[8 + i] = F[i];
+  for (int i = 0; i < NS; i++) {
+    g.hi[i] = R(v[i]);
+    g.lo[i] = kComp ? R(v[i] - (double)g.hi[i]) : R(0);
   }
 }
 
-template <class R, bool kComp>
-PHX_HD R geo_get(const GeoState<R>& g, int i) {
+template <class R, bool kComp, int NS>
+PHX_HD R geo_get(const GeoState<R, NS>& g, int i) {
   return kComp ? g.hi[i] + g.lo[i] : g.hi[i];
 }
 
 // x2 measured from the nearer pole where the integrator folds (FP32), else x2 itself.
-template <class R, bool kComp>
-PHX_HD R pole_x2(const GeoState<R>& g) {
+template <class R, bool kComp, int NS>
+PHX_HD R pole_x2(const GeoState<R, NS>& g) {
   if (kComp && g.hi[2] > R(kHalfPi)) {
     const R pi_hi = R(kPi), pi_lo = R(kPi - (double)R(kPi));
     return (pi_hi - g.hi[2]) + (pi_lo - g.lo[2]);
@@ -62,36 +64,37 @@ PHX_HD R pole_x2(const GeoState<R>& g) {
 // ((d0 + d3) + 2 (d1 + d2)) dt/6 needs two 12-vectors instead of four.  The stage loop is deliberately not unrolled:
 // one copy of the stage body (metric, derivatives, both Christoffel contractions) keeps the march loop small enough
 // for the instruction cache, which four unrolled copies overflow.
-template <class R, bool kComp>
-PHX_HD void rk4_step(R a, R hs, GeoState<R>& g, R dt) {
+template <class R, bool kComp, int NS>
+PHX_HD void rk4_step(R a, R hs, GeoState<R, NS>& g, R dt) {
+  constexpr bool kF = NS == 12;
   const R pi_hi = R(kPi), pi_lo = R(kPi - (double)R(kPi));
   const bool south = kComp && g.hi[2] > R(kHalfPi);
-  R inc[12], s03[12], s12[12];
+  R inc[NS], s03[NS], s12[NS];
 #pragma unroll
-  for (int i = 0; i < 12; i++) inc[i] = R(0);
+  for (int i = 0; i < NS; i++) inc[i] = R(0);
 #pragma unroll 1
   for (int q = 0; q < 4; q++) {
     R y[12];
 #pragma unroll
-    for (int i = 0; i < 12; i++) y[i] = kComp ? g.hi[i] + (g.lo[i] + inc[i]) : g.hi[i] + inc[i];
+    for (int i = 0; i < NS; i++) y[i] = kComp ? g.hi[i] + (g.lo[i] + inc[i]) : g.hi[i] + inc[i];
     if (south) {
       y[2] = (pi_hi - g.hi[2]) + ((pi_lo - g.lo[2]) - inc[2]);
       y[6] = -y[6];
-      y[10] = -y[10];
+      if constexpr (kF) y[10] = -y[10];
     }
     R d[12];
     d[0] = y[4];
     d[1] = y[5];
     d[2] = y[6];
     d[3] = y[7];
-    geodesic_accel(a, hs, y[1], y[2], y + 4, y + 8, d + 4, d + 8);
+    geodesic_accel<R, kF>(a, hs, y[1], y[2], y + 4, y + 8, d + 4, d + 8);
     if (south) {
       d[2] = -d[2];
       d[6] = -d[6];
-      d[10] = -d[10];
+      if constexpr (kF) d[10] = -d[10];
     }
 #pragma unroll
-    for (int i = 0; i < 12; i++) {
+    for (int i = 0; i < NS; i++) {
       if (q == 0) s03[i] = d[i];
       if (q == 1) s12[i] = d[i];
       if (q == 2) s12[i] += d[i];
@@ -100,12 +103,12 @@ PHX_HD void rk4_step(R a, R hs, GeoState<R>& g, R dt) {
     if (q < 3) {
       const R wdt = (q == 2 ? R(1) : R(0.5)) * dt;
 #pragma unroll
-      for (int i = 0; i < 12; i++) inc[i] = wdt * d[i];
+      for (int i = 0; i < NS; i++) inc[i] = wdt * d[i];
     }
   }
   const R dt6 = dt / R(6);
 #pragma unroll
-  for (int i = 0; i < 12; i++) {
+  for (int i = 0; i < NS; i++) {
     const R du = (s03[i] + R(2) * s12[i]) * dt6;
     if (kComp) {
       comp_add(g.hi[i], g.lo[i], du);
@@ -118,24 +121,26 @@ PHX_HD void rk4_step(R a, R hs, GeoState<R>& g, R dt) {
 // FP64 RK4 step of an FP32 compensated state: the pair is widened to double, stepped, and split back.  Out of line
 // (state passed and returned by value): the mixed-precision island is a few percent of the steps, and its FP64 stage
 // body inlined beside the FP32 one would crowd the march loop's instruction cache.
-static PHX_HD_OUTLINE GeoState<float> rk4_step_widened_ool(double a, double hs, GeoState<float> g, double dt) {
-  GeoState<double> w;
+template <int NS>
+PHX_HD_OUTLINE GeoState<float, NS> rk4_step_widened_ool(double a, double hs, GeoState<float, NS> g, double dt) {
+  GeoState<double, NS> w;
 #pragma unroll
-  for (int i = 0; i < 12; i++) {
+  for (int i = 0; i < NS; i++) {
     w.hi[i] = (double)g.hi[i] + (double)g.lo[i];
     w.lo[i] = 0.0;
   }
-  rk4_step<double, false>(a, hs, w, dt);
+  rk4_step<double, false, NS>(a, hs, w, dt);
 #pragma unroll
-  for (int i = 0; i < 12; i++) {
+  for (int i = 0; i < NS; i++) {
     g.hi[i] = (float)w.hi[i];
     g.lo[i] = (float)(w.hi[i] - (double)g.hi[i]);
   }
   return g;
 }
 
-static PHX_HD void rk4_step_widened(double a, double hs, GeoState<float>& g, double dt) {
-  g = rk4_step_widened_ool(a, hs, g, dt);
+template <int NS>
+PHX_HD void rk4_step_widened(double a, double hs, GeoState<float, NS>& g, double dt) {
+  g = rk4_step_widened_ool<NS>(a, hs, g, dt);
 }
 
 // RAPTOR step size (negative: the ray runs backwards from the camera), capped by a quarter of the AMR cell.

@@ -227,37 +227,88 @@ PHX_HD void cov_derivs(const KerrPt<T>& p, T a, Cov<T>* D1, Cov<T>* D2) {
 
 // Right-hand side of the geodesic equation and of the parallel transport of a polarization vector F:
 //   dk^mu/dl = -Gamma^mu_ab k^a k^b,   dF^mu/dl = -Gamma^mu_ab k^a F^b.
-template <class T>
+// kF = false: k only (F and dF are not touched; the polarization then comes from the Walker-Penrose constant).
+template <class T, bool kF = true>
 PHX_HD void geodesic_accel(T a, T hs, T x1, T x2, const T k[4], const T F[4], T dk[4], T dF[4]) {
   const KerrPt<T> p = kerr_point(a, hs, x1, x2);
   Cov<T> D1, D2;
   cov_derivs(p, a, &D1, &D2);
   const Contra<T> u = contra_metric(p, a);
-  T Pk[4], Qk[4], PF[4], QF[4];
+  T Pk[4], Qk[4];
   symv(D1, k, Pk);  // D1 k
   symv(D2, k, Qk);  // D2 k
-  symv(D1, F, PF);  // D1 F
-  symv(D2, F, QF);  // D2 F
   const T kD1k = Pk[0] * k[0] + Pk[1] * k[1] + Pk[2] * k[2] + Pk[3] * k[3];
   const T kD2k = Qk[0] * k[0] + Qk[1] * k[1] + Qk[2] * k[2] + Qk[3] * k[3];
-  const T kD1F = Pk[0] * F[0] + Pk[1] * F[1] + Pk[2] * F[2] + Pk[3] * F[3];
-  const T kD2F = Qk[0] * F[0] + Qk[1] * F[1] + Qk[2] * F[2] + Qk[3] * F[3];
-  T ak[4], aF[4];
-  for (int n = 0; n < 4; n++) {
-    ak[n] = k[1] * Pk[n] + k[2] * Qk[n];
-    aF[n] = T(0.5) * (k[1] * PF[n] + k[2] * QF[n] + F[1] * Pk[n] + F[2] * Qk[n]);
-  }
+  T ak[4];
+  for (int n = 0; n < 4; n++) ak[n] = k[1] * Pk[n] + k[2] * Qk[n];
   ak[1] -= T(0.5) * kD1k;
   ak[2] -= T(0.5) * kD2k;
-  aF[1] -= T(0.5) * kD1F;
-  aF[2] -= T(0.5) * kD2F;
-  T gk[4], gF[4];
+  T gk[4];
   raise(u, ak, gk);
-  raise(u, aF, gF);
-  for (int n = 0; n < 4; n++) {
-    dk[n] = -gk[n];
-    dF[n] = -gF[n];
+  for (int n = 0; n < 4; n++) dk[n] = -gk[n];
+  if constexpr (kF) {
+    T PF[4], QF[4];
+    symv(D1, F, PF);  // D1 F
+    symv(D2, F, QF);  // D2 F
+    const T kD1F = Pk[0] * F[0] + Pk[1] * F[1] + Pk[2] * F[2] + Pk[3] * F[3];
+    const T kD2F = Qk[0] * F[0] + Qk[1] * F[1] + Qk[2] * F[2] + Qk[3] * F[3];
+    T aF[4];
+    for (int n = 0; n < 4; n++) aF[n] = T(0.5) * (k[1] * PF[n] + k[2] * QF[n] + F[1] * Pk[n] + F[2] * Qk[n]);
+    aF[1] -= T(0.5) * kD1F;
+    aF[2] -= T(0.5) * kD2F;
+    T gF[4];
+    raise(u, aF, gF);
+    for (int n = 0; n < 4; n++) dF[n] = -gF[n];
   }
+}
+
+// Walker-Penrose constant of a null geodesic k with a polarization vector f (k.f = 0), in the MKS-BHAC coordinates of
+// this file (Kerr-Schild t and phi, r = exp(x1), theta(x2)):
+//   kappa = (r + i a cos(theta)) (sin(theta) B - i A),
+//   A = R(k) E(f) - R(f) E(k),   B = T(k) P(f) - T(f) P(k),
+//   R(v) = dr(v) = r v^1,   T(v) = dtheta(v) = theta' v^2,   E(v) = v^t - a sin^2(theta) v^phi,
+//   P(v) = (r^2 + a^2) v^phi - a v^t - a dr(v).
+// Y(k, f) = Re kappa and h(k, f) = -Im kappa are the contractions of k and f with Kerr's Killing-Yano 2-form
+// Y = a cos(theta) dr ^ (dt - a sin^2 dphi) + r sin(theta) dtheta ^ ((r^2 + a^2) dphi - a dt) and its Hodge dual, the
+// closed conformal Killing-Yano form h = db, b = [(r^2 + a^2 sin^2) dt - a sin^2 (r^2 + a^2) dphi] / 2 (Boyer-Lindquist
+// forms; the Kerr-Schild change of t and phi adds the -a dr in P).  Both are constant along the geodesic when f is
+// parallel-transported (Walker & Penrose 1970; Chandrasekhar 1983 sec. 63), so kappa taken once at the camera fixes
+// the transported polarization direction at every later point.
+template <class T>
+struct WPForms {
+  T A, B;
+};
+
+template <class T>
+PHX_HD WPForms<T> wp_forms(T a, const KerrPt<T>& p, const T k[4], const T f[4]) {
+  const T rr = p.r * p.r + a * a;
+  const T Rk = p.r * k[1], Rf = p.r * f[1];
+  const T Tk = p.tp * k[2], Tf = p.tp * f[2];
+  const T Ek = k[0] - a * p.s2 * k[3], Ef = f[0] - a * p.s2 * f[3];
+  const T Pk = rr * k[3] - a * k[0] - a * Rk, Pf = rr * f[3] - a * f[0] - a * Rf;
+  return {Rk * Ef - Rf * Ek, Tk * Pf - Tf * Pk};
+}
+
+template <class T>
+PHX_HD void walker_penrose(T a, const KerrPt<T>& p, const T k[4], const T f[4], T kappa[2]) {
+  const WPForms<T> w = wp_forms(a, p, k, f);
+  const T wre = p.s * w.B, wim = -w.A, ac = a * p.c;
+  kappa[0] = p.r * wre - ac * wim;
+  kappa[1] = p.r * wim + ac * wre;
+}
+
+// Components (C, S), up to one common factor, of the transported polarization vector on an orthonormal screen pair
+// (perp, para) orthogonal to k at point p, from the Walker-Penrose constant: f = C perp + S para + alpha k, A and B are
+// linear in f with A(k) = B(k) = 0, and kappa (r - i a cos) = (r^2 + a^2 cos^2) (sin B(f) - i A(f)), a 2x2 system in
+// (C, S) solved by Cramer's rule without the division (cos 2 chi and sin 2 chi need only the ratio).
+template <class T>
+PHX_HD void wp_components(T a, const KerrPt<T>& p, const T k[4], const T perp[4], const T para[4], const T kappa[2],
+                          T* C, T* S) {
+  const WPForms<T> fp = wp_forms(a, p, k, perp), fq = wp_forms(a, p, k, para);
+  const T ac = a * p.c;
+  const T wre = kappa[0] * p.r + kappa[1] * ac, wim = kappa[1] * p.r - kappa[0] * ac;
+  *C = -wre * fq.A - p.s * fq.B * wim;
+  *S = p.s * fp.B * wim + fp.A * wre;
 }
 
 }  // namespace phx

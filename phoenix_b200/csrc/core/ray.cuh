@@ -64,10 +64,10 @@ struct RenderConsts {
   R freq[kMaxFreqs], hconst[kMaxFreqs], jscale[kMaxFreqs];
 };
 
-// The camera set-up of one pixel in FP64: initial photon state (x, k), polarization vector F1 and the sign of the
-// impact parameter beta.
+// The camera set-up of one pixel in FP64: initial photon state (x, k), polarization vector F1, its Walker-Penrose
+// constant kappa and the sign of the impact parameter beta.
 struct RayStart {
-  double ph[8], F1[4];
+  double ph[8], F1[4], kappa[2];
   int bsign;
 };
 
@@ -81,6 +81,8 @@ PHX_HD_OUTLINE RayStart ray_start(const RenderConsts<R>& rc, R a, R hs, int32_t 
   pixel_impact(i, j, rc.W, rc.H, rc.fov_x, rc.fov_y, rc.cos_pa, rc.sin_pa, &alpha, &beta);
   camera_photon(rc.cam, alpha, beta, st.ph);
   camera_pol<R>(a, hs, st.ph, st.F1);
+  const KerrPt<double> pc = kerr_point<double>(a, hs, st.ph[1], st.ph[2]);
+  walker_penrose<double>(a, pc, st.ph + 4, st.F1, st.kappa);
   st.bsign = beta < 0.0 ? -1 : (beta > 0.0 ? 1 : 0);
   return st;
 }
@@ -96,8 +98,14 @@ struct Ray {
   using R = typename Pol::R;
   static constexpr bool kComp = Pol::kComp, kMixed = Pol::kMixed;
   static constexpr bool kLate = M == Mode::kFP64;  // the reference's one-pass-late sample order (see advance())
+  // FP32 and mixed: the polarization direction at a sample comes from the Walker-Penrose constant taken at the camera
+  // (exact for parallel transport), so the geodesic state is (x, k) only; FP64 transports F1 with the state as the
+  // reference does, and follows it bit for bit
+  static constexpr bool kWP = !kLate;
+  static constexpr int kNS = kWP ? 8 : 12;
 
-  GeoState<R> geo;
+  GeoState<R, kNS> geo;
+  R kappa[2];   // Walker-Penrose constant of (k, F1) (kWP)
   R px[4], pk[4], pF[4], pdl;  // FP64 (kLate): the pending sample's point and the length of the step to it
   bool pvalid, terminate;
   int steps, turns, bsign, nplasma, bad;
@@ -119,6 +127,8 @@ struct Ray {
     pix = pixel;
     const RayStart st = ray_start<R>(rc, s.a, s.hs, pixel);
     geo_init<R, kComp>(geo, st.ph, st.F1);
+    kappa[0] = R(st.kappa[0]);
+    kappa[1] = R(st.kappa[1]);
 #pragma unroll
     for (int f = 0; f < NF; f++) acc_reset<R, kMixed>(acc, f);
     pvalid = false;
@@ -162,7 +172,11 @@ struct Ray {
     for (int i = 0; i < 4; i++) {
       cx[i] = geo_get<R, kComp>(geo, i);
       ck[i] = geo_get<R, kComp>(geo, 4 + i);
-      cF[i] = geo_get<R, kComp>(geo, 8 + i);
+      if constexpr (kWP) {
+        cF[i] = R(0);  // unused: the sample takes the polarization from kappa
+      } else {
+        cF[i] = geo_get<R, kComp>(geo, 8 + i);
+      }
     }
     const R r = exp_t(cx[1]);
     const bool alive = r < rc.r_out && r > rc.cut_in && steps < rc.max_steps && !terminate;
@@ -242,8 +256,8 @@ struct Ray {
   PHX_HD void process_sample(const SnapView<R, PT>& s, const RenderConsts<R>& rc, const R x0[4], const R k0[4],
                              const R F0[4], R r, R hl, int right, RayCounters& ctr) {
     R k[4] = {k0[0], k0[1], k0[2], k0[3]};
+    const KerrPt<R> p0 = kerr_point_r(s.a, s.hs, r, x0[2]);  // the sample's own (unwrapped) point
     {
-      const KerrPt<R> p0 = kerr_point_r(s.a, s.hs, r, x0[2]);
       const Cov<R> g0 = cov_metric(p0, s.a);
       if (fabs_t(dot(g0, k, k)) > R(1e-6) && r > R(2)) {
         if constexpr (kMixed) {
@@ -324,10 +338,18 @@ struct Ray {
       cth = mu;
     }
     // polarization axes of the plasma frame with B as reference direction; EVPA rotation from the transported F1
-    R perp[4], para[4], pFd[4];
+    R perp[4], para[4];
     observer_axes_lowered(sqrt_neg_g(p), k, fl.U, fl.B, kd, Ud, Bd, -kU, kB, UB, BB, perp, para);
-    symv(g, F0, pFd);
-    const R C = dot4(pFd, perp), S = dot4(pFd, para);
+    R C, S;
+    if constexpr (kWP) {
+      // the transported F1's components on (perp, para), from kappa at the point the state describes
+      wp_components(s.a, p0, k, perp, para, kappa, &C, &S);
+    } else {
+      R pFd[4];
+      symv(g, F0, pFd);
+      C = dot4(pFd, perp);
+      S = dot4(pFd, para);
+    }
     const R inn = fastm::rcp(C * C + S * S);
     const R c2 = (C * C - S * S) * inn, s2 = R(2) * C * S * inn;
     const R ratio = -kU;  // nu_plasma / nu_camera

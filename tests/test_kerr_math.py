@@ -1,0 +1,104 @@
+"""Host checks of the device geometry code (core/*.cuh compiled by g++): the Walker-Penrose constant that the FP32 and
+mixed kernels use in place of transporting the polarization vector.
+
+Along FP64 geodesics integrated with the kernels' own RK4 (core/geodesic.cuh, F transported as the reference does),
+kappa = (r + i a cos) (sin B - i A) stays constant, and cos 2chi / sin 2chi rebuilt from kappa on an observer's screen
+pair (core/kerr.cuh wp_components) equal those of the transported F.  The rays dive to r ~ 2-4, cross the equator and
+pass within a degree of the pole; the agreement is bounded by the integration error of the transported F itself.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+
+import pytest
+
+from tests.conftest import ROOT
+
+SRC = r"""
+#include <cmath>
+#include <cstdio>
+#include "geodesic.cuh"
+#include "camera.cuh"
+using namespace phx;
+
+// One ray: start point (r0, x2), wave vector direction, polarization guess; steps dl = h r until r leaves [rmin, 1e3].
+static void ray(double a, double r0, double x2, double k1, double k2, double k3, double h, double rmin) {
+  const double hs = 0.25;
+  GeoState<double, 12> g;
+  double x[4] = {0, std::log(r0), x2, 0.3}, k[4] = {0, k1, k2, k3}, f[4] = {0, 0.01, 0.2, 0.05};
+  const KerrPt<double> p = kerr_point(a, hs, x[1], x[2]);
+  const Cov<double> c = cov_metric(p, a);
+  normalize_null(c, k);
+  double kd[4];
+  symv(c, k, kd);
+  f[0] = -(kd[1] * f[1] + kd[2] * f[2] + kd[3] * f[3]) / kd[0];
+  double kap0[2];
+  walker_penrose(a, p, k, f, kap0);
+  for (int i = 0; i < 4; i++) { g.hi[i] = x[i]; g.hi[4 + i] = k[i]; g.hi[8 + i] = f[i]; }
+  for (int i = 0; i < 12; i++) g.lo[i] = 0;
+  double drift = 0, evpa = 0, rlo = 1e30, thlo = 10, thhi = -10;
+  for (int n = 0; n < 20000; n++) {
+    double X[4], K[4], F[4];
+    for (int i = 0; i < 4; i++) { X[i] = g.hi[i]; K[i] = g.hi[4 + i]; F[i] = g.hi[8 + i]; }
+    const KerrPt<double> q = kerr_point(a, hs, X[1], X[2]);
+    const Cov<double> cc = cov_metric(q, a);
+    double kap[2];
+    walker_penrose(a, q, K, F, kap);
+    const double m = std::hypot(kap0[0], kap0[1]);
+    drift = std::fmax(drift, std::hypot(kap[0] - kap0[0], kap[1] - kap0[1]) / m);
+    rlo = std::fmin(rlo, q.r);
+    const double th = std::atan2(q.s, q.c);
+    thlo = std::fmin(thlo, th);
+    thhi = std::fmax(thhi, th);
+    if (cc.tt < -1e-3) {  // a static observer exists: compare the two EVPA routes on its screen
+      double U[4] = {1.0 / std::sqrt(-cc.tt), 0, 0, 0};
+      const double b[4] = {0.0, 0.3, 1.0 / q.tp, 0.2};
+      double perp[4], para[4], om, Fd[4], C2, S2;
+      observer_axes(cc, sqrt_neg_g(q), K, U, b, perp, para, &om);
+      symv(cc, F, Fd);
+      const double C1 = dot4(Fd, perp), S1 = dot4(Fd, para);
+      wp_components(a, q, K, perp, para, kap0, &C2, &S2);
+      const double n1 = C1 * C1 + S1 * S1, n2 = C2 * C2 + S2 * S2;
+      evpa = std::fmax(evpa, std::fabs((C1 * C1 - S1 * S1) / n1 - (C2 * C2 - S2 * S2) / n2));
+      evpa = std::fmax(evpa, std::fabs(2 * C1 * S1 / n1 - 2 * C2 * S2 / n2));
+    }
+    rk4_step<double, false, 12>(a, hs, g, h * q.r);
+    const double rn = std::exp(g.hi[1]);
+    if (rn < rmin || rn > 1e3) break;
+  }
+  std::printf("%.3e %.3e %.4f %.4f %.4f\n", drift, evpa, rlo, thlo, thhi);
+}
+
+int main() {
+  ray(0.9375, 40.0, 0.9, -0.02, 0.0021, 0.0012, 0.002, 1.5);    // dives to r ~ 3.8, into the south, back out
+  ray(0.5, 20.0, 1.4, -0.05, -0.0040, 0.0030, 0.002, 1.5);      // heads north and plunges through the horizon
+  ray(0.99, 30.0, 0.12, -0.03, -0.0015, 0.0004, 0.002, 1.5);    // starts 7 deg from the pole and passes over it
+  ray(0.9375, 12.0, 1.6, -0.04, 0.0002, 0.0070, 0.001, 2.05);   // grazes the photon region near the horizon
+  return 0;
+}
+"""
+
+
+@pytest.fixture(scope="module")
+def wp_results(tmp_path_factory):
+    d = tmp_path_factory.mktemp("wp")
+    src, exe = d / "wp.cpp", d / "wp"
+    src.write_text(SRC)
+    core = os.path.join(ROOT, "phoenix_b200", "csrc", "core")
+    subprocess.check_call(["g++", "-O2", "-std=c++17", "-I" + core, str(src), "-o", str(exe)])
+    out = subprocess.check_output([str(exe)]).decode().split("\n")
+    return [[float(v) for v in line.split()] for line in out if line.strip()]
+
+
+def test_walker_penrose_constant_is_conserved(wp_results):
+    for drift, _, rlo, thlo, thhi in wp_results:
+        assert rlo < 6.0  # every ray reaches the strong-field region
+        assert drift <= 1e-7, (drift, rlo)
+
+
+def test_evpa_from_walker_penrose_matches_transport(wp_results):
+    for _, evpa, *_ in wp_results:
+        assert evpa <= 1e-7, evpa
+    # the set covers both hemispheres and a polar passage
+    assert min(r[3] for r in wp_results) < 0.2 and max(r[4] for r in wp_results) > 1.7
