@@ -42,9 +42,9 @@ FLOPS = dict(step=1800.0, sample=900.0, freq=850.0)
 # its job index (4 B) and one 48 B FreqOut record per frequency.
 BYTES = dict(sample=256.0, step=28.0, ray=4.0, ray_freq=48.0)
 # DRAM bytes (read + write) per ray-step of k_march, from the ncu capture of one launch of this workload
-# (profiles/k_march_plain_gpu_512.md): dram__bytes_read.sum + dram__bytes_write.sum = 801.4 MB over the launch's
+# (profiles/k_march_plain_gpu_512.md): dram__bytes_read.sum + dram__bytes_write.sum = 803.6 MB over the launch's
 # 726.6M ray-steps.  Scaled to the average launch by its ray-steps.
-DRAM_BYTES_PER_STEP = 1.103
+DRAM_BYTES_PER_STEP = 1.106
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 
 
