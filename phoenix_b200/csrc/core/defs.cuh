@@ -59,15 +59,32 @@ PHX_HD void sincos_t(T x, T* s, T* c) {
 #endif
 }
 
+// x mod y for y > 0 and |x / y| < 2^40, bit-identical to fmod: the truncated quotient n makes x - n y exactly
+// representable, so one FMA with n returns it exactly.  The quotient estimate q = trunc(x * (1/y)) is off by at most
+// one; the sign of the remainder (or |r| >= y) shows which, and the FMA is redone with n.
+PHX_HD double fmod_exact(double x, double y) {
+  const double q = trunc(x * (1.0 / y));
+  double r = fma(-q, y, x);
+  if (x >= 0.0) {
+    if (r < 0.0) r = fma(-(q - 1.0), y, x);
+    else if (r >= y) r = fma(-(q + 1.0), y, x);
+  } else {
+    if (r > 0.0) r = fma(-(q + 1.0), y, x);
+    else if (r <= -y) r = fma(-(q - 1.0), y, x);
+  }
+  return r == 0.0 ? copysign(0.0, x) : r;  // fmod's zero carries the sign of x
+}
+
 // x mod y for y > 0 (sign of x kept).  On the device the float form is a truncated-quotient FMA, which is what the
-// reference's device build does (core/numerics/macros.hpp:41); both are exact for the |x| < 4 pi that occur here.
+// reference's device build does (core/numerics/macros.hpp:41), exact for the |x| < 4 pi that occur here; the double
+// form is fmod_exact (the library fmod's bits at a fraction of its cost).
 template <class T>
 PHX_HD T fmod_t(T x, T y) {
 #if defined(__CUDA_ARCH__)
   if constexpr (sizeof(T) == 4) {
     return fmaf(-truncf(x * (1.0f / y)), y, x);
   } else {
-    return fmod(x, y);
+    return fmod_exact(x, y);
   }
 #else
   return std::fmod(x, y);

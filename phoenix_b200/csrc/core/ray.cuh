@@ -282,7 +282,7 @@ struct Ray {
       for (int i = 0; i < 4; i++) xd[i] = (double)geo.hi[i] + (double)geo.lo[i];
       const SnapView<double, PT> sd = s.fp64_view();
       wrap_coords(xd);
-      if (exp_t(xd[1]) < 1.0) return;
+      if (xd[1] < 0.0) return;  // r < 1 (x1 = ln r)
       if (outside_domain(sd, xd)) return;
       if (ig == -1 || !inside_cached(sd, ig, xd)) {
         wrap_coords(xd);

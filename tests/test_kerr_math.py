@@ -1,5 +1,5 @@
 """Host checks of the device geometry code (core/*.cuh compiled by g++): the Walker-Penrose constant that the FP32 and
-mixed kernels use in place of transporting the polarization vector.
+mixed kernels use in place of transporting the polarization vector, and the exact double remainder of the wrap.
 
 Along FP64 geodesics integrated with the kernels' own RK4 (core/geodesic.cuh, F transported as the reference does),
 kappa = (r + i a cos) (sin B - i A) stays constant, and cos 2chi / sin 2chi rebuilt from kappa on an observer's screen
@@ -102,3 +102,53 @@ def test_evpa_from_walker_penrose_matches_transport(wp_results):
         assert evpa <= 1e-7, evpa
     # the set covers both hemispheres and a polar passage
     assert min(r[3] for r in wp_results) < 0.2 and max(r[4] for r in wp_results) > 1.7
+
+
+FMOD_SRC = r"""
+#include <cmath>
+#include <cstdio>
+#include <cstdint>
+#include <cstring>
+#include <initializer_list>
+#include "defs.cuh"
+
+static uint64_t bits(double v) { uint64_t b; std::memcpy(&b, &v, 8); return b; }
+
+int main() {
+  const double ys[2] = {phx::kPi, phx::kTwoPi};
+  uint64_t s = 0x9E3779B97F4A7C15ull, n = 0, bad = 0;
+  auto next = [&]() { s ^= s << 13; s ^= s >> 7; s ^= s << 17; return s; };
+  for (double y : ys) {
+    for (int i = 0; i < 2000000; i++) {
+      const uint64_t u = next();
+      double x;
+      if (i % 4 == 0) {  // within a few ulps of a multiple of y
+        const double m = (double)((int64_t)(u % 401) - 200) * y;
+        x = std::nextafter(m, (u >> 20) & 1 ? 1e300 : -1e300);
+        for (int k = (int)((u >> 21) % 4); k > 0; k--) x = std::nextafter(x, (u >> 23) & 1 ? 1e300 : -1e300);
+      } else {
+        x = ((double)(u >> 11) / 9007199254740992.0 - 0.5) * 1400.0 / (1 + (u % 7));
+      }
+      n++;
+      if (bits(phx::fmod_exact(x, y)) != bits(std::fmod(x, y))) bad++;
+    }
+    for (double x : {0.0, -0.0, y, -y, 2 * y, -3 * y, std::nextafter(y, 0.0), std::nextafter(-y, 0.0)}) {
+      n++;
+      if (bits(phx::fmod_exact(x, y)) != bits(std::fmod(x, y))) bad++;
+    }
+  }
+  std::printf("%llu %llu\n", (unsigned long long)n, (unsigned long long)bad);
+  return 0;
+}
+"""
+
+
+def test_fmod_exact_matches_fmod_bit_for_bit(tmp_path):
+    """The device's double remainder (core/defs.cuh fmod_exact) against the C library's fmod, bit for bit: random
+    arguments up to 700 in magnitude and arguments within a few ulps of multiples of pi and 2 pi."""
+    src, exe = tmp_path / "fm.cpp", tmp_path / "fm"
+    src.write_text(FMOD_SRC)
+    core = os.path.join(ROOT, "phoenix_b200", "csrc", "core")
+    subprocess.check_call(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-I" + core, str(src), "-o", str(exe)])
+    n, bad = map(int, subprocess.check_output([str(exe)]).decode().split())
+    assert n > 4_000_000 and bad == 0, (n, bad)
