@@ -101,7 +101,7 @@ typedef struct {
   int32_t period;      /* march passes between lane refills, 0 = default (64) */
   int32_t blocks_per_sm; /* register-cap variant, as resident warps per SM / 4 (1: up to 255 registers in 128-thread
                             blocks; 3: 168 registers, 4: 128, as one 384 / 512-thread block per SM when the job list
-                            fills every SM, else as 128-thread blocks); 0 = default (FP32 4; mixed, FP64 1) */
+                            fills every SM, else as 128-thread blocks); 0 = default (FP32 4, mixed 3, FP64 1) */
 } PhxRenderParams;
 
 /* What a render reports (a superset of the reference's device::Info, src/device/kernel.cuh:23-30). */
@@ -208,7 +208,7 @@ typedef struct {
 
 typedef struct {
   int32_t tile_rays;       /* rays per queue tile, 0 = 32 */
-  int32_t blocks_per_sm;   /* register-cap variant (FP32: 1, 3, 4; mixed 1, 3), 0 = default (FP32 4, else 1) or autotuned */
+  int32_t blocks_per_sm;   /* register-cap variant (FP32: 1, 3, 4; mixed 1, 3), 0 = default (FP32 4, mixed 3, FP64 1) or autotuned */
   int32_t period;          /* march passes between lane refills, 0 = default 64 or autotuned */
   int32_t autotune;        /* nonzero: time every (blocks_per_sm, period) candidate on a sample of the batch's tiles
                               at creation and keep the fastest */
@@ -269,7 +269,7 @@ typedef struct {
   int32_t max_freqs;      /* frequency slots per request (1 or 4; FP32 also up to 32), default 4 */
   int32_t tile_rays;      /* rays per queue tile, default 32 */
   int32_t period;         /* march passes between lane refills, default 64 */
-  int32_t blocks_per_sm;  /* register-cap variant, 0 = default (FP32 4, else 1) */
+  int32_t blocks_per_sm;  /* register-cap variant, 0 = default (FP32 4, mixed 3, FP64 1) */
   int32_t max_items;      /* requests per run of the kernel before the queue is recycled, default 4096 */
   int64_t max_tiles;      /* tiles per run of the kernel, a power of two, default 2^22 */
   int32_t idle_ns;        /* sleep of an idle warp between polls of the queue, default 2000 */

@@ -290,7 +290,8 @@ PhxBatch* create_batch(const PhxBatchItem* items, int32_t nitems, const PhxBatch
   ck(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "cudaStreamCreate");
   ck(cudaEventCreate(&b->e0), "cudaEventCreate");
   ck(cudaEventCreate(&b->e1), "cudaEventCreate");
-  b->shape = {o.blocks_per_sm > 0 ? o.blocks_per_sm : (b->precision == PHX_PREC_FP32 ? 4 : 1),
+  b->shape = {o.blocks_per_sm > 0 ? o.blocks_per_sm
+                                  : (b->precision == PHX_PREC_FP32 ? 4 : b->precision == PHX_PREC_MIXED ? 3 : 1),
              o.period > 0 ? o.period : phx::kDefaultPeriod};
   if (o.autotune && b->ntrial > 0) autotune(b.get());
   capture(b.get());

@@ -195,10 +195,11 @@ struct QueueShape {
   int period;
 };
 
-// Default register-cap variant (measured on B200): FP32 128 registers (16 warps per SM), mixed and FP64 uncapped.
+// Default register-cap variant (measured on B200): FP32 128 registers (16 warps per SM), mixed 168 (12 warps), FP64
+// uncapped.
 template <Mode M>
 constexpr int default_queue_blocks_per_sm() {
-  return M == Mode::kFP32 ? 4 : 1;
+  return M == Mode::kFP32 ? 4 : M == Mode::kMixed ? 3 : 1;
 }
 
 // Launches the queue kernel for `nf_slots` frequency slots (1, 4 or 32) on a persistent grid (resident blocks x SMs),
