@@ -28,7 +28,6 @@ PHX_HD void comp_add(R& hi, R& lo, R d) {
 
 template <class R, int NS = 12>
 struct GeoState {
-  static constexpr int kN = NS;
   R hi[NS];  // x[0..3], k[4..7], F[8..11] (NS = 12)
   R lo[NS];  // compensation (FP32 only)
 };
