@@ -114,11 +114,12 @@ struct Ray {
   int32_t pix;
   int leaf;     // leaf of the last step-size lookup (-1: none), tested before the leaf map
   R idxc[3];    // its inverse cell sizes
-  // transfer records (4x4 operator, Stokes sums, optical depths) per frequency slot: the mixed kernels of up to 4 slots
-  // keep them in the block's dynamic shared memory (kSmemPerThread bytes per thread), the others in registers.
-  // Measured on B200: mixed 3-frequency renders 14% faster (the FP64 island's registers no longer spill); FP32 with
-  // one slot 3% slower, with four unchanged.
-  static constexpr bool kAccShared = (kMixed || M == Mode::kFP64) && NF <= 4;
+  // transfer records (4x4 operator, Stokes sums, optical depths) per frequency slot: the kernels of 4 slots and the
+  // mixed and FP64 kernels of 1 keep them in the block's dynamic shared memory (kSmemPerThread bytes per thread), the
+  // FP32 one-slot and all 32-slot kernels in registers.  Measured on B200: mixed 3-frequency renders 14% faster (the
+  // FP64 island's registers no longer spill), FP64 3-5%, FP32 3-frequency 3-6% (no spills at 128 registers); FP32
+  // with one slot 3% slower, so it keeps registers.
+  static constexpr bool kAccShared = (kMixed || M == Mode::kFP64 || NF > 1) && NF <= 4;
   using AccStore = std::conditional_t<kAccShared, AccShared<R, kMixed, NF>, AccRegs<R, kMixed, NF>>;
   static constexpr size_t kSmemPerThread = AccStore::kSmemPerThread;
   AccStore acc;
