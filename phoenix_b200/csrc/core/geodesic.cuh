@@ -59,15 +59,33 @@ PHX_HD R pole_x2(const GeoState<R, NS>& g) {
   return g.hi[2] + (kComp ? g.lo[2] : R(0));
 }
 
+// exp(d) for |d| <= 0.1 by its Taylor series to d^11 (truncation below 3e-21 relative).
+template <class T>
+PHX_HD T exp_small(T d) {
+  T e = T(1);
+#pragma unroll
+  for (int n = 11; n >= 1; n--) e = T(1) + d * T(1.0 / n) * e;
+  return e;
+}
+
 // One classical RK4 step of length dt.  Stage sums are kept as (d0 + d3) and (d1 + d2) so that the update
 // ((d0 + d3) + 2 (d1 + d2)) dt/6 needs two 12-vectors instead of four.  The stage loop is deliberately not unrolled:
 // one copy of the stage body (metric, derivatives, both Christoffel contractions) keeps the march loop small enough
 // for the instruction cache, which four unrolled copies overflow.
-template <class R, bool kComp, int NS>
+// kShift (uncompensated state only): each stage's exp(x1) and sincos(x2) come from the step's starting point and short
+// series of the stage offset (exp_small, sincos_small: exact to rounding for the offsets allowed), one exp and one
+// sincos per step instead of four; a stage whose offset is larger evaluates the point directly.
+template <class R, bool kComp, int NS, bool kShift = false>
 PHX_HD void rk4_step(R a, R hs, GeoState<R, NS>& g, R dt) {
   constexpr bool kF = NS == 12;
+  static_assert(!(kShift && kComp), "the shifted stages need an uncompensated state");
   const R pi_hi = R(kPi), pi_lo = R(kPi - (double)R(kPi));
   const bool south = kComp && g.hi[2] > R(kHalfPi);
+  R e0 = R(0), sx0 = R(0), cx0 = R(0);
+  if constexpr (kShift) {
+    e0 = exp_t(g.hi[1]);
+    sincos_t(g.hi[2], &sx0, &cx0);
+  }
   R inc[NS], s03[NS], s12[NS];
 #pragma unroll
   for (int i = 0; i < NS; i++) inc[i] = R(0);
@@ -86,7 +104,19 @@ PHX_HD void rk4_step(R a, R hs, GeoState<R, NS>& g, R dt) {
     d[1] = y[5];
     d[2] = y[6];
     d[3] = y[7];
-    geodesic_accel<R, kF>(a, hs, y[1], y[2], y + 4, y + 8, d + 4, d + 8);
+    if constexpr (kShift) {
+      const R d1 = inc[1], d2 = inc[2];
+      if (fabs_t(d1) <= R(0.1) && fabs_t(d2) <= R(0.5)) {
+        R sd, cd;
+        sincos_small(d2, &sd, &cd);
+        const KerrPt<R> p = kerr_point_rsc(a, hs, e0 * exp_small(d1), y[2], sx0 * cd + cx0 * sd, cx0 * cd - sx0 * sd);
+        geodesic_accel_at<R, kF>(a, p, y + 4, y + 8, d + 4, d + 8);
+      } else {
+        geodesic_accel<R, kF>(a, hs, y[1], y[2], y + 4, y + 8, d + 4, d + 8);
+      }
+    } else {
+      geodesic_accel<R, kF>(a, hs, y[1], y[2], y + 4, y + 8, d + 4, d + 8);
+    }
     if (south) {
       d[2] = -d[2];
       d[6] = -d[6];
@@ -128,7 +158,7 @@ PHX_HD_OUTLINE GeoState<float, NS> rk4_step_widened_ool(double a, double hs, Geo
     w.hi[i] = (double)g.hi[i] + (double)g.lo[i];
     w.lo[i] = 0.0;
   }
-  rk4_step<double, false, NS>(a, hs, w, dt);
+  rk4_step<double, false, NS, true>(a, hs, w, dt);
 #pragma unroll
   for (int i = 0; i < NS; i++) {
     g.hi[i] = (float)w.hi[i];

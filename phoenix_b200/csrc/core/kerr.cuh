@@ -76,14 +76,12 @@ PHX_HD void sincos_small(T d, T* sn, T* cs) {
   *cs = c;
 }
 
-// Geometry at (r, x2) when r = exp(x1) is already known.
+// Geometry at (r, x2) when r = exp(x1) and sin x2, cos x2 are already known.
 template <class T>
-PHX_HD KerrPt<T> kerr_point_r(T a, T hs, T r, T x2) {
+PHX_HD KerrPt<T> kerr_point_rsc(T a, T hs, T r, T x2, T sx, T cx) {
   KerrPt<T> p;
   p.r = r;
-  // sin 2x2, cos 2x2 from one sincos of x2 (double-angle identities)
-  T sx, cx;
-  sincos_t(x2, &sx, &cx);
+  // sin 2x2, cos 2x2 from sin x2, cos x2 (double-angle identities)
   const T s2x = T(2) * sx * cx, c2x = (cx - sx) * (cx + sx);
   const T d = T(0.5) * hs * s2x;  // theta = x2 + d
   p.tp = T(1) + hs * c2x;
@@ -102,6 +100,14 @@ PHX_HD KerrPt<T> kerr_point_r(T a, T hs, T r, T x2) {
   p.isig = fastm::rcp(p.sig);  // FP32: hardware reciprocal (2 ulp), FP64: exact division
   p.q = T(2) * p.r * p.isig;
   return p;
+}
+
+// Geometry at (r, x2) when r = exp(x1) is already known.
+template <class T>
+PHX_HD KerrPt<T> kerr_point_r(T a, T hs, T r, T x2) {
+  T sx, cx;
+  sincos_t(x2, &sx, &cx);
+  return kerr_point_rsc(a, hs, r, x2, sx, cx);
 }
 
 template <class T>
@@ -229,8 +235,7 @@ PHX_HD void cov_derivs(const KerrPt<T>& p, T a, Cov<T>* D1, Cov<T>* D2) {
 //   dk^mu/dl = -Gamma^mu_ab k^a k^b,   dF^mu/dl = -Gamma^mu_ab k^a F^b.
 // kF = false: k only (F and dF are not touched; the polarization then comes from the Walker-Penrose constant).
 template <class T, bool kF = true>
-PHX_HD void geodesic_accel(T a, T hs, T x1, T x2, const T k[4], const T F[4], T dk[4], T dF[4]) {
-  const KerrPt<T> p = kerr_point(a, hs, x1, x2);
+PHX_HD void geodesic_accel_at(T a, const KerrPt<T>& p, const T k[4], const T F[4], T dk[4], T dF[4]) {
   Cov<T> D1, D2;
   cov_derivs(p, a, &D1, &D2);
   const Contra<T> u = contra_metric(p, a);
@@ -260,6 +265,11 @@ PHX_HD void geodesic_accel(T a, T hs, T x1, T x2, const T k[4], const T F[4], T 
     raise(u, aF, gF);
     for (int n = 0; n < 4; n++) dF[n] = -gF[n];
   }
+}
+
+template <class T, bool kF = true>
+PHX_HD void geodesic_accel(T a, T hs, T x1, T x2, const T k[4], const T F[4], T dk[4], T dF[4]) {
+  geodesic_accel_at<T, kF>(a, kerr_point(a, hs, x1, x2), k, F, dk, dF);
 }
 
 // Walker-Penrose constant of a null geodesic k with a polarization vector f (k.f = 0), in the MKS-BHAC coordinates of
