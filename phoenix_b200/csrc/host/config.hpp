@@ -1,8 +1,13 @@
-// config.toml + command-line overrides, with the reference's key set and semantics (src/host/io/config.hpp:35-381):
-// a TOML subset (sections, key = value, "#" comments outside double quotes, quoted strings), `section.key=value`
-// overrides where any camera.frequenc* override first removes every frequency form of the file, typed required and
-// optional keys, exactly one frequency form (single, list, linspace, logspace) with duplicates detected by their
-// "%e" spelling (they name the HDF5 datasets), and an error for any unknown key.  Error messages are the reference's.
+// config.toml + command-line overrides for the PHOENIX command line.  The accepted keys, their meaning, the override
+// syntax and the error messages are the reference renderer's (src/host/io/config.hpp:35-381), so that its config
+// files and scripts keep working:
+//   * a TOML subset: [section] headers, key = value, '#' comments outside double quotes, "quoted" strings; a key
+//     given twice is an error;
+//   * `section.key=value` overrides; an override of any camera.frequenc* key first drops every frequency form the
+//     file gave;
+//   * exactly one frequency form: frequency, frequency_list [a, b, ...], frequency_linspace / frequency_logspace
+//     [start, stop, n]; duplicate frequencies (by their "%e" spelling, which names the HDF5 datasets) are an error;
+//   * typed required and optional keys; every missing required key is listed; any key not in the table is an error.
 #pragma once
 
 #include <map>
@@ -25,12 +30,13 @@ struct RunConfig {
   std::vector<double> frequencies;
 };
 
-// Throws std::runtime_error("Line N: ...") on malformed input.
-void parse_toml(const std::string& text, std::map<std::string, std::string>& kv);
+// Flat "section.key" -> raw value map of a config text.  Throws std::runtime_error("Line N: ...") on malformed input.
+std::map<std::string, std::string> parse_toml(const std::string& text);
 
-// Reads the frequency form of `kv` into `out` (marks the key used). Throws std::runtime_error.
-void read_frequencies(const std::map<std::string, std::string>& kv, std::vector<std::string>& used,
-                      std::vector<double>& out);
+// The frequencies of the one frequency form present in `kv`; its key is appended to `consumed`.
+// Throws std::runtime_error with the reference's messages.
+std::vector<double> read_frequencies(const std::map<std::string, std::string>& kv,
+                                     std::vector<std::string>& consumed);
 
 // Loads `path`, applies the overrides, validates.  Throws std::runtime_error with the reference's messages.
 RunConfig load_config(const std::string& path, const std::vector<std::string>& overrides);

@@ -67,6 +67,44 @@ def test_config_errors(built, cfg, over, msg):
     assert msg in r.stderr
 
 
+REF_FP64 = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
+                        "ref_render_fp64")
+
+
+@pytest.mark.skipif(not os.path.exists(REF_FP64), reason="the reference's CPU build (oracle/_ref) is not built here")
+@pytest.mark.parametrize("over", [
+    ["bogus.key=1"], ["camera.frequency_list=[230e9, 2.3e11]"], ["camera.frequency_linspace=[1e9, 2e9]"],
+    ["camera.frequency_linspace=[1e9, 2e9, 2.5]"], ["camera.frequency_logspace=[3e9, 2e9, 4]"],
+    ["camera.frequency=abc"], ["camera.frequency_list=230e9"], ["camera.frequency_list=[]"],
+    ["camera.frequency_list=[1e9, x]"], ["camera.frequency_list=[1e9, -2e9]"], ["output.image=png"],
+    ["output.block_size=0"], ["plasma.beta_c=0"], ["noequals"],
+    ["camera.frequency=1e9", "camera.frequency_list=[2e9]"],
+    ["camera.frequency_list=[1e9,2e9]", "camera.frequency_list=[3e9, 3e9]"],
+])
+def test_config_errors_match_reference(built, cfg, over):
+    """The same config and overrides give the reference's own parser (host/io/config.hpp, compiled into its CPU
+    build) and ours the same error text."""
+    ours = _run(built, [cfg] + over)
+    ref = subprocess.run([REF_FP64, cfg] + over, capture_output=True, text=True)
+    assert ours.returncode == 1 and ref.returncode == 1
+    what = ref.stderr.strip().split("ref_render: ", 1)[1]
+    assert what in ours.stderr
+
+
+@pytest.mark.skipif(not os.path.exists(REF_FP64), reason="the reference's CPU build (oracle/_ref) is not built here")
+def test_config_file_errors_match_reference(built, tmp_path, cfg):
+    text = open(cfg).read()
+    bad = tmp_path / "bad.toml"
+    for variant in (text.replace("[camera]", "[camera"), text + "\n[camera]\ninclination = 3\n",
+                    text.replace("mass = ", "#mass = ").replace("rt_outer = ", "#rt_outer = "),
+                    text.replace("mass = ", "mass ")):
+        bad.write_text(variant)
+        ours = _run(built, [str(bad)])
+        ref = subprocess.run([REF_FP64, str(bad)], capture_output=True, text=True)
+        assert ours.returncode == 1 and ref.returncode == 1
+        assert ref.stderr.strip().split("ref_render: ", 1)[1] in ours.stderr
+
+
 def test_config_file_errors(built, tmp_path, cfg):
     text = open(cfg).read()
     bad = tmp_path / "bad.toml"
