@@ -29,6 +29,7 @@ sys.path.insert(0, ROOT)
 
 GEN = os.path.join(ROOT, "phoenix_b200", "_build", "phx_gen_snapshot")
 REF_CPU = os.path.join(ROOT, "oracle", "_ref", "ref_render_fp32")
+REF_CPU64 = os.path.join(ROOT, "oracle", "_ref", "ref_render_fp64")
 REF_GPU = os.path.join(ROOT, "oracle", "_ref", "ref_gpu_fp32")
 
 WORKLOAD = dict(base=(192, 96, 96), nlevels=3, refine=(3.5, 25.0, 0.55), seed=0, img=512,
@@ -41,10 +42,13 @@ FLOPS = dict(step=1800.0, sample=900.0, freq=850.0)
 # of the trilinear gather (256 B); per step the flattened leaf-map entry (4 B) and the leaf's lb/dxc (24 B); per ray
 # its job index (4 B) and one 48 B FreqOut record per frequency.
 BYTES = dict(sample=256.0, step=28.0, ray=4.0, ray_freq=48.0)
-# DRAM bytes (read + write) per ray-step of k_march, from the ncu capture of one launch of this workload
-# (profiles/k_march_plain_gpu_512.md): dram__bytes_read.sum + dram__bytes_write.sum = 803.6 MB over the launch's
-# 726.6M ray-steps.  Scaled to the average launch by its ray-steps.
+# DRAM bytes (read + write) per ray-step of k_march, from an ncu capture of one launch of this workload (the 60 deg
+# image): dram__bytes_read.sum + dram__bytes_write.sum = 803.6 MB over the launch's 726.6M ray-steps.  Scaled to the
+# average launch by its ray-steps.
 DRAM_BYTES_PER_STEP = 1.106
+# FMA-pipe share of active cycles of k_march on this workload (ncu sm__pipe_fma_cycles_active.avg.pct_of_peak_
+# sustained_active, one launch of the 60 deg image).
+FMA_PIPE_ACTIVE = 0.449
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 
 
@@ -157,21 +161,74 @@ def _cpu_passes(dump, grid, w, stride, ncores, repeat, tmp):
         out = subprocess.check_output([REF_CPU, cfg, "--pixels", pfile, "--threads", str(ncores), "--inclinations",
                                        ",".join(str(i) for i in w["inclinations"]), "--repeat", str(repeat)])
         passes = [json.loads(l) for l in out.decode().splitlines() if l.strip()]
-        return "reference", pix.size * len(w["inclinations"]), [(p["steps"], p["seconds"]) for p in passes]
+        return "reference", pix.size * len(w["inclinations"]), [(p["steps"], p["seconds"], p["nplasma"])
+                                                                  for p in passes]
     from oracle.oracle import Oracle
     os_ = [Oracle(dump, grid, inclination=i, img_width=w["img"], img_height=w["img"], frequencies=(w["frequency"],),
                   m_unit=w["m_unit"], nlevels=w["nlevels"]) for i in w["inclinations"]]
     passes = []
     for _ in range(repeat):
-        st_sum, sec = 0, 0.0
+        st_sum, sec, np_sum = 0, 0.0, 0
         for o in os_:
             _, st, secs = o.render(pix, threads=ncores)
             st_sum += int(st[:, 0].sum())
+            np_sum += int(st[:, 1].sum())
             sec += secs
-        passes.append((st_sum, sec))
+        passes.append((st_sum, sec, np_sum))
     for o in os_:
         o.close()
     return "port", pix.size * len(w["inclinations"]), passes
+
+
+def _ref_config(tmp, dump, grid, w, inclination):
+    from tests.golden.cases import write_config
+    case = dict(snapshot="cfg1", inclination=inclination, img_width=w["img"], img_height=w["img"],
+                frequencies=[w["frequency"]], m_unit=w["m_unit"])
+    cfg = os.path.join(tmp, "c.toml")
+    write_config(cfg, case, dump, grid, tmp)
+    with open(cfg) as f:
+        text = f.read().replace("nlevels = 3", f"nlevels = {w['nlevels']}")
+    with open(cfg, "w") as f:
+        f.write(text)
+    return cfg
+
+
+def oracle_errors(dump, grid, w, images, stride, threads=0):
+    """Errors of the rendered images against the FP64 oracle on a strided pixel sample (the reference's own FP64 CPU
+    build, oracle/_ref, or the FP64 C oracle port where that build is absent): per image the sample's total-flux
+    error (I relative to I; Q, U, V relative to I) and per-pixel L1 / Linf of I.  images: [W*H, 1, 6] arrays in the
+    order of w["inclinations"]."""
+    ncores = threads or os.cpu_count()
+    pix = np.arange(0, w["img"] * w["img"], stride, dtype=np.int64)
+    pix = ((pix + (pix // w["img"]) * 7) % (w["img"] * w["img"])).astype(np.int32)
+    out = []
+    t0 = time.time()
+    with tempfile.TemporaryDirectory() as tmp:
+        pfile = os.path.join(tmp, "pix.bin")
+        pix.tofile(pfile)
+        for incl, res in zip(w["inclinations"], images):
+            if os.path.exists(REF_CPU64):
+                kind = "reference FP64 CPU build (oracle/_ref)"
+                ofile = os.path.join(tmp, "out.bin")
+                subprocess.check_output([REF_CPU64, _ref_config(tmp, dump, grid, w, incl), "--pixels", pfile,
+                                         "--out", ofile, "--threads", str(ncores)])
+                ref = np.fromfile(ofile, dtype=np.float64).reshape(pix.size, 6)
+            else:
+                from oracle.oracle import Oracle
+                kind = "FP64 C oracle port"
+                o = Oracle(dump, grid, inclination=incl, img_width=w["img"], img_height=w["img"],
+                           frequencies=(w["frequency"],), m_unit=w["m_unit"], nlevels=w["nlevels"])
+                ref = o.render(pix, threads=ncores)[0].reshape(pix.size, 6)
+                o.close()
+            got = np.asarray(res).reshape(-1, 6)[pix]
+            I, Ir = got[:, 0], ref[:, 0]
+            sI = Ir.sum()
+            out.append({"inclination": incl, "flux_I": float(abs(I.sum() - sI) / abs(sI)),
+                        "flux_QUV": float(max(abs(got[:, q].sum() - ref[:, q].sum()) for q in (1, 2, 3)) / abs(sI)),
+                        "l1_I": float(np.abs(I - Ir).sum() / np.abs(Ir).sum()),
+                        "linf_I": float(np.abs(I - Ir).max() / np.abs(Ir).max())})
+    return {"sample": f"every {stride}th pixel of each {w['img']}^2 image ({pix.size} pixels), {kind}",
+            "images": out, "seconds": time.time() - t0}
 
 
 def cpu_stride(dump, grid, w, ncores, tmp, seconds_target=10.0):
@@ -184,7 +241,7 @@ def cpu_baseline(dump, grid, w, threads=0, repeat=1, stride=None):
     """The reference's own CPU path (its FP32 build, OpenMP over all host threads) -- or the FP64 C oracle port when
     the reference could not be compiled -- on a strided pixel sample of the workload's three images, sized by a short
     calibration run to about 10 s of pixel-loop wall time per pass.
-    Returns (ray-steps/s per pass list, cores, kind, description)."""
+    Returns (ray-steps/s per pass list, cores, kind, description, [(steps, seconds, emitting samples) per pass])."""
     ncores = threads or os.cpu_count()
     with tempfile.TemporaryDirectory() as tmp:
         stride = stride or cpu_stride(dump, grid, w, ncores, tmp)
@@ -192,7 +249,7 @@ def cpu_baseline(dump, grid, w, threads=0, repeat=1, stride=None):
     desc = (f"{npix} rays per pass (every {stride}th pixel of each {w['img']}^2 image, 3 inclinations), "
             f"{'reference FP32 CPU build (oracle/_ref)' if kind == 'reference' else 'FP64 C oracle port'}, "
             f"{ncores} OpenMP threads, pixel-loop wall time")
-    return [st / sec for st, sec in passes], ncores, kind, desc, passes
+    return [p[0] / p[1] for p in passes], ncores, kind, desc, passes
 
 
 def run_reference(args):
@@ -205,6 +262,7 @@ def run_reference(args):
     timed = passes[args.warmup:]
     steps = sum(p[0] for p in timed)
     secs = sum(p[1] for p in timed)
+    emitting = sum(p[2] for p in timed) / max(steps, 1)
     value = steps / secs
     line = {"metric": "ray-steps/s", "value": value, "unit": "ray-steps/s", "n_gpus": args.gpus, "steps": K,
             "warmup": args.warmup, "ms_per_step": 1e3 * secs / K, "higher_is_better": True,
@@ -212,7 +270,8 @@ def run_reference(args):
             "config": {"workload": "plain GPU path: 192x96x96 base grid, 8^3 blocks, 3 AMR levels (15.6M cells), "
                                    "3 x 512^2 images at 10/60/163 deg, 230 GHz, m_unit 1.2e18",
                        "sample": desc},
-            "cpu_baseline": {"value": value, "unit": "ray-steps/s", "cores": cores, "kind": kind, "sample": desc},
+            "cpu_baseline": {"value": value, "unit": "ray-steps/s", "cores": cores, "kind": kind, "sample": desc,
+                             "emitting_samples_per_step": emitting},
             "e2e": {"value": value, "unit": "ray-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -686,6 +745,8 @@ def main():
         for k, p in enumerate(params):
             snap.render_async(p, jobs.data_ptr(), npix, res[k].data_ptr(), ctr[k].data_ptr(), 0, stream.cuda_stream)
 
+    # the FP32 roofline's denominator, measured on this GPU before the timed region
+    fp32_peak = P.measure_fp32_peak() if rank == 0 else 0.0
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             one_step()
@@ -752,8 +813,6 @@ def main():
         kavg_s = sum(kms) / nlaunch * 1e-3
         flops = FLOPS["step"] * steps_total + (FLOPS["sample"] + nfreq * FLOPS["freq"]) * nplasma_total
         fp32_achieved = flops / nlaunch / kavg_s / 1e12
-        props = torch.cuda.get_device_properties(dev)
-        fp32_peak = props.multi_processor_count * 128 * 2 * 1.965e9 / 1e12
         rays = nimg * npix
         nbytes = (BYTES["sample"] * nplasma_total + BYTES["step"] * steps_total +
                   (BYTES["ray"] + nfreq * BYTES["ray_freq"]) * rays)
@@ -774,26 +833,32 @@ def main():
             "rays_per_s": nimg * npix / (ms_max * 1e-3) * world,
             "ray_steps_per_step": steps_total / args.steps,
             "ray_steps_per_launch": steps_per_launch,
+            "emitting_samples_per_step": nplasma_total / max(steps_total, 1),
             "gpu_launches": nlaunch,
-            "roofline": {"bound": "hbm", "achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s",
-                         "frac": hbm_achieved / hbm_peak, "traffic": traffic,
-                         "kernel": "k_march", "launch_ms": kavg_s * 1e3, "algorithmic_bytes_per_launch": nbytes / nlaunch,
-                         "note": f"secondary roofline ({peak_kind} HBM copy peak): the bytes the march requests "
-                                 "(256 B gather per emitting sample, 28 B leaf lookup per step, 52 B per ray) per "
-                                 "launch over the CUDA-event launch time; most hit L1/L2, traffic is the DRAM share. "
-                                 "The kernel is FP32-issue bound: see roofline_fp32"},
-            "roofline_fp32": {"bound": "fp32", "achieved": fp32_achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                              "frac": fp32_achieved / fp32_peak,
-                              "note": "algorithmic flops per launch (1800 per step, 900 per emitting sample, 850 per "
-                                      "sample-frequency) over the launch time; peak = SMs x 128 FP32 lanes x 2 x "
-                                      "1965 MHz (nominal, no measured FP32 peak for this pool)"},
+            "roofline": {"bound": "fp32", "achieved": fp32_achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                         "frac": fp32_achieved / fp32_peak, "traffic": traffic, "kernel": "k_march",
+                         "launch_ms": kavg_s * 1e3, "flops_per_launch": flops / nlaunch,
+                         "flops_per_unit": FLOPS, "fma_pipe_active": FMA_PIPE_ACTIVE,
+                         "note": "the march is bound by FP32 instruction issue: algorithmic FP32 flops per launch "
+                                 "(per ray-step, per emitting sample, per sample-frequency) over the CUDA-event launch "
+                                 "time; peak = FP32 FMA issue rate measured on this GPU in this run "
+                                 "(phx_measure_fp32_peak); traffic = DRAM bytes per launch; fma_pipe_active = the "
+                                 "FMA-pipe share of cycles from ncu on this workload"},
+            "roofline_hbm": {"bound": "hbm", "achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s",
+                             "frac": hbm_achieved / hbm_peak, "traffic": traffic,
+                             "algorithmic_bytes_per_launch": nbytes / nlaunch,
+                             "note": f"secondary roofline ({peak_kind} HBM copy peak): the bytes the march requests "
+                                     "(256 B gather per emitting sample, 28 B leaf lookup per step, 52 B per ray) per "
+                                     "launch over the CUDA-event launch time; most hit L1/L2, traffic is the DRAM "
+                                     "share"},
             "clocks": clocks,
             "e2e": e2e,
         }
         if world == 1 and not args.no_cpu:
-            rates, cores, kind, desc, _ = cpu_baseline(dump, grid, w)
+            rates, cores, kind, desc, cpass = cpu_baseline(dump, grid, w)
             line["cpu_baseline"] = {"value": rates[0], "unit": "ray-steps/s", "cores": cores, "kind": kind,
-                                    "sample": desc}
+                                    "sample": desc, "emitting_samples_per_step": cpass[0][2] / max(cpass[0][0], 1)}
+            line["oracle_errors"] = oracle_errors(dump, grid, w, [r.cpu().numpy() for r in res], stride=10)
         print(json.dumps(line), flush=True)
     snap.close()
     if world > 1:

@@ -37,8 +37,9 @@ enum {
 enum {
   PHX_PREC_FP32 = 0,  /* FP32 throughout after the FP64 camera set-up */
   PHX_PREC_FP64 = 1,  /* FP64 throughout */
-  PHX_PREC_MIXED = 2  /* FP32 bulk, FP64 near the horizon, in the null renormalisation, for large-depth segment
-                         operators, and Kahan-summed Stokes vectors */
+  PHX_PREC_MIXED = 2  /* FP64 geodesic (state, RK4, step size, placement of samples in leaves and cells), FP32
+                         plasma stage with FP64 null renormalisation, FP64 segment operators at large depth and
+                         Kahan-summed Stokes vectors */
 };
 
 /* Snapshot creation flags. */
@@ -95,7 +96,7 @@ typedef struct {
   double m_unit, r_low, r_high, beta_c, sigma_cut, thetae_min, thetae_max, rt_outer;
   /* this library */
   int32_t precision;   /* PHX_PREC_* */
-  double r_fp64;       /* mixed: FP64 RK4 inside r < r_fp64 * r_horizon (<= 0: default 3, the photon-orbit region) */
+  double r_fp64;       /* unused (kept for layout; the mixed mode integrates every step in FP64) */
   double tau_fp64;     /* mixed: FP64 segment operator where h max|K| exceeds this (<= 0: default 0.1) */
   int32_t block;       /* unused (the block shape follows blocks_per_sm; PhxRenderInfo.block reports it) */
   int32_t period;      /* march passes between lane refills, 0 = default (64) */
@@ -183,12 +184,28 @@ int phx_render_async(PhxSnapshot* s, const PhxRenderParams* p, const int32_t* d_
  * PHX_NOALLOC_MAX_JOBS job slots (4 MiB), which every GPU that loads the library holds until the process exits.
  * d_res: device buffer of img_width * img_height * nfreqs records.  Asynchronous on `stream` (NULL = default).
  * Rejects njobs > PHX_NOALLOC_MAX_JOBS with PHX_E_INVALID.  The first call on a device resolves the array's
- * device address with that device current; make that first call before any stream capture.  All calls share the
+ * device address with that device current; make that first call before any stream capture.  The address is kept for
+ * the life of the process: do not call this entry point again on a device after cudaDeviceReset (the reset unloads
+ * the library's module, and the kept address would be stale).  All calls share the
  * array (it keeps the last call's contents; the counter block is cleared before each launch), so calls that overlap
  * on the GPU race. */
 #define PHX_NOALLOC_MAX_JOBS (1 << 20)
 int phx_render_noalloc(PhxSnapshot* s, const PhxRenderParams* p, const int32_t* jobs, int64_t njobs,
                        PhxFreqOut* d_res, void* stream);
+
+/* Per-frequency image totals of a device-resident result, computed on the device (the reference's
+ * host::output::compute_spec and compute_tau, src/host/io/output.hpp:43-74): the flux line's I, Q, U, V [Jy] over
+ * the pixels whose I+Q+U+V is finite, and the spectrum file's mean tau and tauF over the pixels whose six values are
+ * finite.  Lets a caller that only wants the spectrum skip the image download (48 bytes per pixel and frequency). */
+typedef struct {
+  double IQUV[4];            /* total flux [Jy] */
+  double tau_mean, tauF_mean;
+  int64_t n_flux, n_tau;     /* pixels in the flux sums and in the optical-depth means */
+} PhxSpectrum;
+
+/* Reduces d_res (img_width * img_height * nfreqs records on the device, 16-byte aligned) into d_spec (nfreqs device
+ * records), asynchronously on `stream` (NULL = default).  Allocates nothing; deterministic (fixed summation order). */
+int phx_spectrum_async(const PhxRenderParams* p, const PhxFreqOut* d_res, PhxSpectrum* d_spec, void* stream);
 
 /* ---- Batches: many images in one persistent, graph-captured launch ----
  * No single reference counterpart: the reference renders one image per device::render call
@@ -246,6 +263,10 @@ int phx_batch_result(PhxBatch* b, int32_t item, PhxFreqOut* res, PhxRenderInfo* 
 /* Device address of item `item`'s records (valid until phx_batch_destroy). */
 int phx_batch_device_result(PhxBatch* b, int32_t item, PhxFreqOut** d_res);
 
+/* Item `item`'s per-frequency totals (nfreqs records in host memory), reduced on the device from the batch's last
+ * run without downloading the image (see phx_spectrum_async).  Synchronous on the batch's stream. */
+int phx_batch_spectrum(PhxBatch* b, int32_t item, PhxSpectrum* spec);
+
 int phx_batch_tuning(const PhxBatch* b, PhxBatchTuning* t);
 
 void phx_batch_destroy(PhxBatch* b);
@@ -294,6 +315,8 @@ typedef struct {
   int64_t rays, steps;
   int64_t snapshot_bytes, table_bytes, arena_bytes, arena_used, job_table_bytes;
   int32_t grid, regs;
+  int64_t idle_exits;  /* kernel runs that ended by their bounded idle wait (idle_limit polls) */
+  int64_t retries;     /* requests put back in the queue because the kernel ended before finishing them */
 } PhxServerStats;
 
 void phx_default_server_options(PhxServerOptions* o);
@@ -326,6 +349,11 @@ void phx_server_destroy(PhxServer* s);
  * per frequency.  The directory must exist. */
 int phx_write_output(const PhxRenderParams* p, const PhxFreqOut* res, const char* outdir, const char* image,
                      int32_t block_size, double* flux);
+
+/* No counterpart in the reference.  Measures the current GPU's FP32 issue rate [TFLOP/s] with independent FMA chains
+ * on every SM (best of `repeats` timed launches after one warm-up): the measured denominator of the raymarch's FP32
+ * roofline, taken on the box and at the clocks of the run that reports it. */
+int phx_measure_fp32_peak(int32_t repeats, double* tflops);
 
 /* Description of the last error on this host thread. */
 const char* phx_last_error(void);

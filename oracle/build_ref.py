@@ -10,7 +10,9 @@ system is not used.  Instead its hot-path headers are compiled where they lie wi
                                       ACCURACY=FP32 (the reference's CUDA path, src/device/kernel.cu:284-360)
 
 Outputs go to oracle/_ref/ only (git-ignored; they travel with the working tree).  Nothing is built when the reference
-tree is absent.  Usage: python oracle/build_ref.py [--src /path/to/reference] [--no-gpu]
+tree is absent.  The tree is taken from --src, else from the PHX_REFERENCE_SRC environment variable, else from a
+checkout named `reference` beside this repository.
+Usage: python oracle/build_ref.py [--src /path/to/reference] [--no-gpu]
 """
 from __future__ import annotations
 
@@ -22,15 +24,21 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-DEFAULT_SRC = "/root/reference"
+
+
+def default_src() -> str:
+    """PHX_REFERENCE_SRC, else a `reference` checkout next to the repository."""
+    env = os.environ.get("PHX_REFERENCE_SRC")
+    return env if env else os.path.normpath(os.path.join(HERE, os.pardir, os.pardir, "reference"))
 
 
 def _newer(target: str, deps) -> bool:
     return os.path.exists(target) and all(os.path.getmtime(target) >= os.path.getmtime(d) for d in deps)
 
 
-def build(src: str = DEFAULT_SRC, gpu: bool = True, verbose: bool = False) -> dict:
+def build(src: str = "", gpu: bool = True, verbose: bool = False) -> dict:
     built = {}
+    src = src or default_src()
     inc = os.path.join(src, "src")
     if not os.path.isdir(inc):
         return built
@@ -63,7 +71,7 @@ def build(src: str = DEFAULT_SRC, gpu: bool = True, verbose: bool = False) -> di
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--src", default=DEFAULT_SRC)
+    ap.add_argument("--src", default="")
     ap.add_argument("--no-gpu", action="store_true")
     a = ap.parse_args()
     res = build(a.src, gpu=not a.no_gpu, verbose=True)

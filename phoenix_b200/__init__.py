@@ -16,7 +16,7 @@ from . import native
 from .native import (CTR, NUM_COUNTERS, PREC_FP32, PREC_FP64, PREC_MIXED, PhxError, PhxRenderInfo, make_params,
                      schedule_morton, write_output)
 
-__all__ = ["Snapshot", "Batch", "Server", "make_params", "schedule_morton", "write_output", "flux", "pixel_solid_angle", "PhxError", "PREC_FP32",
+__all__ = ["Snapshot", "Batch", "Server", "make_params", "schedule_morton", "write_output", "flux", "pixel_solid_angle", "device_spectrum", "spectrum_rows", "measure_fp32_peak", "PhxError", "PREC_FP32",
            "PREC_FP64", "PREC_MIXED", "CTR", "NUM_COUNTERS"]
 
 G_GRAV, M_SUN, C_LIGHT, KPC, JANSKY = 6.674e-8, 1.989e33, 2.99792458e10, 3.086e21, 1e23
@@ -170,6 +170,13 @@ class Batch:
         native.check(native.lib().phx_batch_result(self._h, item, res.ctypes.data, C.byref(info)))
         return res, info.as_dict()
 
+    def spectrum(self, item: int) -> np.ndarray:
+        """Item's per-frequency totals reduced on the device: rows (I, Q, U, V [Jy], mean tau, mean tauF)."""
+        p = self.params[item]
+        spec = (native.PhxSpectrum * p.nfreqs)()
+        native.check(native.lib().phx_batch_spectrum(self._h, item, spec))
+        return spectrum_rows(spec)
+
     def device_result(self, item: int) -> int:
         ptr = C.c_void_p()
         native.check(native.lib().phx_batch_device_result(self._h, item, C.byref(ptr)))
@@ -263,6 +270,23 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def spectrum_rows(spec) -> np.ndarray:
+    """PhxSpectrum records as rows (I, Q, U, V [Jy], mean tau, mean tauF)."""
+    return np.array([list(r.IQUV) + [r.tau_mean, r.tauF_mean] for r in spec], dtype=np.float64)
+
+
+def device_spectrum(params, d_res: int, d_spec: int, stream: int = 0):
+    """phx_spectrum_async on device pointers: nfreqs PhxSpectrum records (64 bytes each) into d_spec."""
+    native.check(native.lib().phx_spectrum_async(C.byref(params), d_res, d_spec, stream or None))
+
+
+def measure_fp32_peak(repeats: int = 5) -> float:
+    """The current GPU's measured FP32 FMA issue rate [TFLOP/s] (phx_measure_fp32_peak)."""
+    v = C.c_double()
+    native.check(native.lib().phx_measure_fp32_peak(repeats, C.byref(v)))
+    return v.value
 
 
 def pixel_solid_angle(p) -> float:

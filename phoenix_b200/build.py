@@ -37,7 +37,7 @@ DEVICE_SRC = ["device/march_fp64_f64.cu", "device/march_fp64_f32.cu", "device/ma
               "device/march_mixed_nf1.cu", "device/march_mixed_nf4.cu", "device/march_dispatch.cu", "device/capi.cu",
               "device/queue_fp32_nf1.cu", "device/queue_fp32_nf4.cu", "device/queue_mixed.cu", "device/queue_fp64.cu",
               "device/queue_dispatch.cu", "device/batch.cu", "device/server.cu",
-              "device/decode.cu"]
+              "device/decode.cu", "device/spectrum.cu", "device/peak.cu"]
 HOST_SRC = ["host/snapshot.cpp", "host/output.cpp", "host/hdf5_writer.cpp"]
 CLI_SRC = ["host/main.cpp", "host/config.cpp"]
 

@@ -2,21 +2,23 @@
 //
 // Ray::advance() performs one pass of the reference's per-pixel loop (core/render/pixel.hpp:179-211): view the
 // state -> liveness test -> leaf lookup -> a plasma sample -> theta turning points -> grid-capped step size -> RK4
-// step.  FP64 processes the previous point's sample, as the reference does; the FP32 paths process this point's
-// (see advance() for why both give the same samples).
+// step.  FP64 processes the previous point's sample, as the reference does; the FP32 and mixed paths process this
+// point's (see advance() for why both give the same samples).
 // Because the state is explicit, a warp can retire a finished ray and start a new one in the same lane while its
 // neighbours keep marching (the kernel's lane refill), instead of idling until the warp's longest ray ends.
 //
-// Precision policies:
-//   FP32   float everywhere after the FP64 camera set-up; compensated (hi, lo) geodesic state with south-pole
-//          folding; deviation-form transfer operator.
-//   FP64   double everywhere.
-//   Mixed  FP32 bulk plus FP64 islands: RK4 steps inside r < r_fp64 (default 3 r_horizon), the null-condition
-//          renormalisation of each sample's wave vector, the segment operator where h max|K| > tau_fp64 (large
-//          optical / Faraday depth per segment), Kahan summation of the Stokes vector, and the placement of samples
-//          in leaves and cells (the compensated FP32 position widened to FP64 against FP64 leaf geometry).  The last
-//          island removes the dominant FP32 error: the reference's interpolation is block-local, so a sample that FP32
-//          rounding moves across a block face picks up the neighbour block's values.
+// Each mode has two precisions: G of the geodesic (state, RK4, step size, leaf placement) and R of the plasma stage
+// (interpolated fluid, synchrotron coefficients, transfer operator).
+//   FP32   G = R = float after the FP64 camera set-up; compensated (hi, lo) geodesic state with south-pole folding;
+//          deviation-form transfer operator.
+//   FP64   G = R = double.
+//   Mixed  G = double, R = float, plus FP64 islands of the plasma stage: the null-condition renormalisation of each
+//          sample's wave vector, the segment operator where h max|K| > tau_fp64 (large optical / Faraday depth per
+//          segment) and Kahan summation of the Stokes vector.  The geodesic is FP64 because the reference's
+//          interpolation is block-local (no ghost cells): the sampled fluid jumps where a ray crosses a block face, so a
+//          sample that the FP32 trajectory error (1e-7 .. 1e-6 in x after thousands of steps) carries across a face
+//          picks up the neighbour block's values.  With an FP64 trajectory and FP64 step sizes the samples sit where
+//          the FP64 oracle's do.
 #pragma once
 
 #include <type_traits>
@@ -35,20 +37,31 @@ enum class Mode : int { kFP32 = 0, kFP64 = 1, kMixed = 2 };
 
 template <Mode M>
 struct Policy;
+// R: plasma-stage precision; G: geodesic precision; kComp: compensated (hi, lo) geodesic state; kShift: RK4 stages
+// take exp(x1) and sincos(x2) from the step's start point and short series of the stage offset.
 template <>
 struct Policy<Mode::kFP32> {
   using R = float;
-  static constexpr bool kComp = true, kMixed = false;
+  using G = float;
+  static constexpr bool kComp = true, kMixed = false, kShift = false;
 };
 template <>
 struct Policy<Mode::kFP64> {
   using R = double;
-  static constexpr bool kComp = false, kMixed = false;
+  using G = double;
+  static constexpr bool kComp = false, kMixed = false, kShift = false;
 };
 template <>
 struct Policy<Mode::kMixed> {
   using R = float;
-  static constexpr bool kComp = true, kMixed = true;
+  using G = double;
+  static constexpr bool kComp = false, kMixed = true, kShift = true;
+};
+
+// Integration limits and step-size constants in the precision G of a geodesic.
+template <class G>
+struct StepConsts {
+  G stepsize, inv_stepsize, r_out, cut_in, rt_outer, tiny, big;
 };
 
 // Render-wide constants (one image: camera, integration, plasma and frequencies).
@@ -57,11 +70,20 @@ struct RenderConsts {
   int32_t W, H, nfreqs, max_steps, max_order;
   double fov_x, fov_y, cos_pa, sin_pa;
   CameraSpec cam;
-  R stepsize, inv_stepsize, r_out, cut_in, rt_outer;
-  R step_tiny, step_big;
-  R r_fp64, tau_fp64;
+  StepConsts<R> step;         // geodesics in the render precision (FP32, FP64)
+  StepConsts<double> step_d;  // the mixed mode's FP64 geodesic
+  R tau_fp64;
   PlasmaView<R> pv;
   R freq[kMaxFreqs], hconst[kMaxFreqs], jscale[kMaxFreqs];
+
+  template <class G>
+  PHX_HD const StepConsts<G>& steps_in() const {
+    if constexpr (sizeof(G) == sizeof(R)) {
+      return step;
+    } else {
+      return step_d;
+    }
+  }
 };
 
 // The camera set-up of one pixel in FP64: initial photon state (x, k), polarization vector F1, its Walker-Penrose
@@ -73,14 +95,15 @@ struct RayStart {
 
 // Kept out of line: it runs once per ray, and its FP64 code (impact parameters, the Newton solve for x2, the camera
 // tetrad) inlined into the march loop would crowd the loop's instruction cache and register allocation.
-template <class R>
-PHX_HD_OUTLINE RayStart ray_start(const RenderConsts<R>& rc, R a, R hs, int32_t pixel) {
+// G: the precision of the camera tetrad's arithmetic (the geodesic precision, as in the reference's builds).
+template <class G, class R>
+PHX_HD_OUTLINE RayStart ray_start(const RenderConsts<R>& rc, G a, G hs, int32_t pixel) {
   RayStart st;
   const int i = pixel / rc.H, j = pixel % rc.H;
   double alpha, beta;
   pixel_impact(i, j, rc.W, rc.H, rc.fov_x, rc.fov_y, rc.cos_pa, rc.sin_pa, &alpha, &beta);
   camera_photon(rc.cam, alpha, beta, st.ph);
-  camera_pol<R>(a, hs, st.ph, st.F1);
+  camera_pol<G>(a, hs, st.ph, st.F1);
   const KerrPt<double> pc = kerr_point<double>(a, hs, st.ph[1], st.ph[2]);
   walker_penrose<double>(a, pc, st.ph + 4, st.F1, st.kappa);
   st.bsign = beta < 0.0 ? -1 : (beta > 0.0 ? 1 : 0);
@@ -96,7 +119,8 @@ template <Mode M, class PT, int NF>
 struct Ray {
   using Pol = Policy<M>;
   using R = typename Pol::R;
-  static constexpr bool kComp = Pol::kComp, kMixed = Pol::kMixed;
+  using G = typename Pol::G;
+  static constexpr bool kComp = Pol::kComp, kMixed = Pol::kMixed, kShift = Pol::kShift;
   static constexpr bool kLate = M == Mode::kFP64;  // the reference's one-pass-late sample order (see advance())
   // FP32 and mixed: the polarization direction at a sample comes from the Walker-Penrose constant taken at the camera
   // (exact for parallel transport), so the geodesic state is (x, k) only; FP64 transports F1 with the state as the
@@ -104,30 +128,43 @@ struct Ray {
   static constexpr bool kWP = !kLate;
   static constexpr int kNS = kWP ? 8 : 12;
 
-  GeoState<R, kNS> geo;
+  GeoState<G, kNS> geo;
   R kappa[2];   // Walker-Penrose constant of (k, F1) (kWP)
-  R px[4], pk[4], pF[4], pdl;  // FP64 (kLate): the pending sample's point and the length of the step to it
+  G px[4], pk[4], pF[4], pdl;  // FP64 (kLate): the pending sample's point and the length of the step to it
   bool pvalid, terminate;
   int steps, turns, bsign, nplasma, bad;
-  R thdot_prev, dl_prev;
-  R pr;         // radius of the pending sample (exp of px[1], from the step that made it)
+  G thdot_prev, dl_prev;
+  G pr;         // radius of the pending sample (exp of px[1], from the step that made it)
   int32_t pix;
   int leaf;     // leaf of the last step-size lookup (-1: none), tested before the leaf map
-  R idxc[3];    // its inverse cell sizes
+  G idxc[3];    // its inverse cell sizes (FP32 and mixed step-size cap)
   // transfer records (4x4 operator, Stokes sums, optical depths) per frequency slot: the kernels of 4 slots and the
   // mixed and FP64 kernels of 1 keep them in the block's dynamic shared memory (kSmemPerThread bytes per thread), the
-  // FP32 one-slot and all 32-slot kernels in registers.  Measured on B200: mixed 3-frequency renders 14% faster (the
-  // FP64 island's registers no longer spill), FP64 3-5%, FP32 3-frequency 3-6% (no spills at 128 registers); FP32
-  // with one slot 3% slower, so it keeps registers.
+  // FP32 one-slot and all 32-slot kernels in registers.  Measured on B200: mixed 3-frequency renders 14% faster,
+  // FP64 3-5%, FP32 3-frequency 3-6% (no spills at 128 registers); FP32 with one slot 3% slower, so it keeps
+  // registers.
   static constexpr bool kAccShared = (kMixed || M == Mode::kFP64 || NF > 1) && NF <= 4;
   using AccStore = std::conditional_t<kAccShared, AccShared<R, kMixed, NF>, AccRegs<R, kMixed, NF>>;
   static constexpr size_t kSmemPerThread = AccStore::kSmemPerThread;
   AccStore acc;
 
-  PHX_HD void init(const SnapView<R, PT>& s, const RenderConsts<R>& rc, int32_t pixel) {
+  // The snapshot in the geodesic's precision: the plasma-stage view itself (FP32, FP64) or the FP64 view sd (mixed).
+  // Both live in kernel parameter space or in the item table, so no copy is made for the out-of-line callees that
+  // take the view by reference.
+  PHX_HD static const SnapView<G, PT>& geo_view(const SnapView<R, PT>& s, const SnapView<double, PT>& sd) {
+    if constexpr (sizeof(G) == sizeof(R)) {
+      return s;
+    } else {
+      return sd;
+    }
+  }
+
+  PHX_HD void init(const SnapView<R, PT>& s, const SnapView<double, PT>& sd, const RenderConsts<R>& rc,
+                   int32_t pixel) {
     pix = pixel;
-    const RayStart st = ray_start<R>(rc, s.a, s.hs, pixel);
-    geo_init<R, kComp>(geo, st.ph, st.F1);
+    const SnapView<G, PT>& sg = geo_view(s, sd);
+    const RayStart st = ray_start<G>(rc, sg.a, sg.hs, pixel);
+    geo_init<G, kComp>(geo, st.ph, st.F1);
     kappa[0] = R(st.kappa[0]);
     kappa[1] = R(st.kappa[1]);
 #pragma unroll
@@ -136,23 +173,25 @@ struct Ray {
     terminate = false;
     steps = turns = nplasma = bad = 0;
     bsign = st.bsign;
-    thdot_prev = dl_prev = R(0);
-    pr = R(0);
+    thdot_prev = dl_prev = G(0);
+    pr = G(0);
     leaf = -1;
-    idxc[0] = idxc[1] = idxc[2] = R(0);
+    idxc[0] = idxc[1] = idxc[2] = G(0);
   }
 
   // The leaf of the wrapped point xw (the last one first: a ray stays tens of steps in one leaf, and since the
   // leaves tile the domain a point inside it has no other leaf); -1 outside the domain.  Also keeps the leaf's
-  // inverse cell sizes for the FP32 step-size cap.
-  PHX_HD int lookup(const SnapView<R, PT>& s, const R xw[4], RayCounters& ctr) {
+  // inverse cell sizes for the step-size cap of the FP32 and mixed paths.
+  PHX_HD int lookup(const SnapView<G, PT>& s, const G xw[4], RayCounters& ctr) {
     if (leaf >= 0 && inside_leaf(s, leaf, xw, leaf_nudge(xw))) return leaf;
     bool scanned = false;
     const int L = find_leaf(s, xw, &scanned);
     ctr.scans += scanned;
-    if (L >= 0 && L != leaf) {
+    if constexpr (!kLate) {
+      if (L >= 0 && L != leaf) {
 #pragma unroll
-      for (int d = 0; d < 3; d++) idxc[d] = fastm::rcp(ldg(s.dxc + 3 * L + d));  // feeds only the step cap
+        for (int d = 0; d < 3; d++) idxc[d] = fastm::rcp(ldg(s.dxc + 3 * L + d));  // feeds only the step cap
+      }
     }
     leaf = L;
     return L;
@@ -162,40 +201,43 @@ struct Ray {
   //
   // The reference processes each point's plasma sample one pass late (core/render/pixel.hpp:179-211), after the
   // next point's leaf lookup, whose leaf then seeds the sampler's cache check.  FP64 keeps that order, so that it
-  // follows the reference bit for bit.  The FP32 paths process each sample at its own point, before the step, seeded
-  // by its own leaf (found for the step-size cap anyway): the samples, their order and their segment lengths are the
-  // same (points 1.. of the live path inside rt_outer, each with the length of the step that led to it), no copy of
-  // the previous point's state is carried (fewer registers), and the leaf found differs only for points within the
-  // sampler's 1e-9 nudge of a block face, which FP32 positions do not resolve anyway.
-  PHX_HD bool advance(const SnapView<R, PT>& s, const RenderConsts<R>& rc, RayCounters& ctr) {
-    R cx[4], ck[4], cF[4];
+  // follows the reference bit for bit.  The FP32 and mixed paths process each sample at its own point, before the
+  // step, seeded by its own leaf (found for the step-size cap anyway): the samples, their order and their segment
+  // lengths are the same (points 1.. of the live path inside rt_outer, each with the length of the step that led to
+  // it), no copy of the previous point's state is carried (fewer registers), and the leaf found differs only for
+  // points within the sampler's 1e-9 nudge of a block face.
+  PHX_HD bool advance(const SnapView<R, PT>& s, const SnapView<double, PT>& sd, const RenderConsts<R>& rc,
+                      RayCounters& ctr) {
+    const SnapView<G, PT>& sg = geo_view(s, sd);
+    const StepConsts<G>& sc = rc.template steps_in<G>();
+    G cx[4], ck[4], cF[4];
 #pragma unroll
     for (int i = 0; i < 4; i++) {
-      cx[i] = geo_get<R, kComp>(geo, i);
-      ck[i] = geo_get<R, kComp>(geo, 4 + i);
+      cx[i] = geo_get<G, kComp>(geo, i);
+      ck[i] = geo_get<G, kComp>(geo, 4 + i);
       if constexpr (kWP) {
-        cF[i] = R(0);  // unused: the sample takes the polarization from kappa
+        cF[i] = G(0);  // unused: the sample takes the polarization from kappa
       } else {
-        cF[i] = geo_get<R, kComp>(geo, 8 + i);
+        cF[i] = geo_get<G, kComp>(geo, 8 + i);
       }
     }
-    const R r = exp_t(cx[1]);
-    const bool alive = r < rc.r_out && r > rc.cut_in && steps < rc.max_steps && !terminate;
+    const G r = exp_t(cx[1]);
+    const bool alive = r < sc.r_out && r > sc.cut_in && steps < rc.max_steps && !terminate;
     // beyond rt_outer the reference keeps no sample (derive_fluid and process_sample both require r < rt_outer) and
     // caps no step by the grid
-    const bool inner = alive && r < rc.rt_outer;
+    const bool inner = alive && r < sc.rt_outer;
     int L = -1;
     if constexpr (kLate) {
-      const bool pend_plasma = pvalid && pr < rc.rt_outer;
+      const bool pend_plasma = pvalid && pr < sc.rt_outer;
       const bool need_leaf = pend_plasma && alive;
       int right = -1;
       if (need_leaf || inner) {
-        R xw[4] = {cx[0], cx[1], cx[2], cx[3]};
+        G xw[4] = {cx[0], cx[1], cx[2], cx[3]};
         wrap_coords(xw);
-        L = lookup(s, xw, ctr);
-        if (need_leaf) right = (r < R(1) || outside_domain(s, xw)) ? -1 : L;  // wrapping keeps x1: exp(xw[1]) = r
+        L = lookup(sg, xw, ctr);
+        if (need_leaf) right = (r < G(1) || outside_domain(sg, xw)) ? -1 : L;  // wrapping keeps x1: exp(xw[1]) = r
       }
-      if (pend_plasma) process_sample(s, rc, px, pk, pF, pr, pdl, right, ctr);
+      if (pend_plasma) process_sample(s, sg, rc, px, pk, pF, pr, pdl, right, ctr);
 #pragma unroll
       for (int i = 0; i < 4; i++) {
         px[i] = cx[i];
@@ -209,118 +251,88 @@ struct Ray {
     } else {
       if (!alive) return false;
       if (inner) {
-        R xw[4] = {cx[0], cx[1], cx[2], cx[3]};
+        G xw[4] = {cx[0], cx[1], cx[2], cx[3]};
         wrap_coords(xw);
-        L = lookup(s, xw, ctr);
+        L = lookup(sg, xw, ctr);
         if (steps >= 1) {
-          const int right = (r < R(1) || outside_domain(s, xw)) ? -1 : L;  // wrapping keeps x1: exp(xw[1]) = r
-          process_sample(s, rc, cx, ck, cF, r, dl_prev, right, ctr);
+          const int right = (r < G(1) || outside_domain(sg, xw)) ? -1 : L;  // wrapping keeps x1: exp(xw[1]) = r
+          process_sample(s, sg, rc, cx, ck, cF, r, dl_prev, right, ctr);
         }
       }
     }
 
-    if (thdot_prev * ck[2] < R(0) && steps > 2) turns++;
+    if (thdot_prev * ck[2] < G(0) && steps > 2) turns++;
     thdot_prev = ck[2];
     if ((bsign < 0 && turns > rc.max_order) || (bsign > 0 && turns > rc.max_order + 1)) terminate = true;
 
     const bool cap = inner && L >= 0;
-    const R x2 = pole_x2<R, kComp>(geo);
-    R dl;
-    if constexpr (sizeof(R) == 4) {
-      dl = step_size_fast(rc.stepsize, rc.inv_stepsize, x2, ck, cap ? idxc : (const R*)nullptr, rc.step_tiny,
-                          rc.step_big);
+    const G x2 = pole_x2<G, kComp>(geo);
+    G dl;
+    if constexpr (!kLate) {
+      // FP32 and mixed: the reciprocals folded (two divisions instead of twelve; the same rule up to rounding)
+      dl = step_size_fast(sc.stepsize, sc.inv_stepsize, x2, ck, cap ? idxc : (const G*)nullptr, sc.tiny, sc.big);
     } else {
-      R dxcv[3];
+      G dxcv[3];
       if (cap) {
 #pragma unroll
-        for (int d = 0; d < 3; d++) dxcv[d] = ldg(s.dxc + 3 * L + d);
+        for (int d = 0; d < 3; d++) dxcv[d] = ldg(sg.dxc + 3 * L + d);
       }
-      dl = step_size(rc.stepsize, x2, ck, cap ? dxcv : (const R*)nullptr, rc.step_tiny, rc.step_big);
+      dl = step_size(sc.stepsize, x2, ck, cap ? dxcv : (const G*)nullptr, sc.tiny, sc.big);
     }
-    if constexpr (kMixed) {
-      if (r < rc.r_fp64) {
-        rk4_step_widened((double)s.a, (double)s.hs, geo, (double)dl);
-        ctr.fp64_steps++;
-      } else {
-        rk4_step<R, kComp>(s.a, s.hs, geo, dl);
-      }
-    } else {
-      rk4_step<R, kComp>(s.a, s.hs, geo, dl);
-    }
+    rk4_step<G, kComp, kNS, kShift>(sg.a, sg.hs, geo, dl);
+    if constexpr (kMixed) ctr.fp64_steps++;
     dl_prev = fabs_t(dl);
     steps++;
     return true;
   }
 
   // The plasma stage of the sample at point (x0, k0, F0) of radius r, reached by a step of length hl (the reference's
-  // process_sample, core/render/pixel.hpp:52-123).
-  PHX_HD void process_sample(const SnapView<R, PT>& s, const RenderConsts<R>& rc, const R x0[4], const R k0[4],
-                             const R F0[4], R r, R hl, int right, RayCounters& ctr) {
-    R k[4] = {k0[0], k0[1], k0[2], k0[3]};
-    const KerrPt<R> p0 = kerr_point_r(s.a, s.hs, r, x0[2]);  // the sample's own (unwrapped) point
+  // process_sample, core/render/pixel.hpp:52-123).  The point comes in the geodesic's precision G; the fluid,
+  // coefficients and transfer operator run in R.
+  PHX_HD void process_sample(const SnapView<R, PT>& s, const SnapView<G, PT>& sg, const RenderConsts<R>& rc,
+                             const G x0[4], const G k0[4], const G F0[4], G r, G hl, int right, RayCounters& ctr) {
+    // null-condition renormalisation of the sample's wave vector, in the geodesic's precision (reference:
+    // geodesic.hpp:297-306, applied when |k.k| > 1e-6 and r > 2)
+    G kg[4] = {k0[0], k0[1], k0[2], k0[3]};
+    const KerrPt<G> pg = kerr_point_r(sg.a, sg.hs, r, x0[2]);  // the sample's own (unwrapped) point
     {
-      const Cov<R> g0 = cov_metric(p0, s.a);
-      if (fabs_t(dot(g0, k, k)) > R(1e-6) && r > R(2)) {
-        if constexpr (kMixed) {
-          const KerrPt<double> pd = kerr_point((double)s.a, (double)s.hs, (double)x0[1], (double)x0[2]);
-          const Cov<double> gd = cov_metric(pd, (double)s.a);
-          double kd[4] = {k[0], k[1], k[2], k[3]};
-          normalize_null(gd, kd);
-          k[0] = R(kd[0]);
-        } else {
-          normalize_null(g0, k);
-        }
-      }
+      const Cov<G> g0 = cov_metric(pg, sg.a);
+      if (fabs_t(dot(g0, kg, kg)) > G(1e-6) && r > G(2)) normalize_null(g0, kg);
     }
-    // sampler (sampler.hpp:387-427): wrap, domain, cached leaf or a fresh lookup of the re-wrapped point
-    R x[4] = {x0[0], x0[1], x0[2], x0[3]};
+    // sampler (sampler.hpp:387-427): wrap, domain, cached leaf or a fresh lookup of the re-wrapped point, cell and
+    // weights -- all in G; the weighted sum of the primitives in R
+    G xg[4] = {x0[0], x0[1], x0[2], x0[3]};
     int ig = right;
+    wrap_coords(xg);
+    if (r < G(1)) return;  // exp(xg[1]): wrapping keeps x1
+    if (outside_domain(sg, xg)) return;
+    if (ig == -1 || !inside_cached(sg, ig, xg)) {
+      wrap_coords(xg);
+      bool scanned = false;
+      ig = find_leaf(sg, xg, &scanned);
+      ctr.scans += scanned;
+    }
+    if (ig == -1) return;
     R q[kNPrim];
     if constexpr (kMixed) {
-      // the compensated position of this point (mixed processes samples before the step: the state is this point's)
-      double xd[4];
-#pragma unroll
-      for (int i = 0; i < 4; i++) xd[i] = (double)geo.hi[i] + (double)geo.lo[i];
-      const SnapView<double, PT> sd = s.fp64_view();
-      wrap_coords(xd);
-      if (xd[1] < 0.0) return;  // r < 1 (x1 = ln r)
-      if (outside_domain(sd, xd)) return;
-      if (ig == -1 || !inside_cached(sd, ig, xd)) {
-        wrap_coords(xd);
-        bool scanned = false;
-        ig = find_leaf(sd, xd, &scanned);
-        ctr.scans += scanned;
-      }
-      if (ig == -1) return;
-      // cell and weights from the FP64 position; the weighted sum of the FP32 primitives stays FP32
       int c[3];
-      double dd[3];
-      cell_weights<double, PT, true>(sd, ig, xd, c, dd);
+      G dd[3];
+      cell_weights<G, PT, true>(sg, ig, xg, c, dd);
       const R del[3] = {R(dd[0]), R(dd[1]), R(dd[2])};
       gather_prims<R, PT>(s.prim, s.cells, s.nx, ig, c, del, q);
-#pragma unroll
-      for (int i = 0; i < 4; i++) x[i] = R(xd[i]);
     } else {
-      wrap_coords(x);
-      if (r < R(1)) return;  // exp(x[1]): wrapping keeps x1
-      if (outside_domain(s, x)) return;
-      if (ig == -1 || !inside_cached(s, ig, x)) {
-        wrap_coords(x);
-        bool scanned = false;
-        ig = find_leaf(s, x, &scanned);
-        ctr.scans += scanned;
-      }
-      if (ig == -1) return;
-      interp_prims<R, PT, !kComp>(s, ig, x, q);
+      interp_prims<R, PT, !kComp>(s, ig, xg, q);
     }
-    // (FP32 paths: x1 is the sample's own, so exp(x[1]) = r; the mixed path moved x to the FP64 placement)
-    const R rx = kMixed ? exp_t(x[1]) : r;
-    const KerrPt<R> p = kerr_point_r(s.a, s.hs, rx, x[2]);
+    // the rest in R, at the wrapped point (x1 unchanged by the wrap, so its radius is r)
+    const R x2w = R(xg[2]);
+    const R rx = R(r);
+    R k[4] = {R(kg[0]), R(kg[1]), R(kg[2]), R(kg[3])};
+    const KerrPt<R> p = kerr_point_r(s.a, s.hs, rx, x2w);
     const Cov<R> g = cov_metric(p, s.a);
     const Contra<R> u = contra_metric(p, s.a);
     Fluid<R> fl;
     if (!derive_fluid(rc.pv, s.gam, rx, g, u, q, &fl)) return;
-    if (!(r < rc.rt_outer)) return;
+    if (!(r < rc.template steps_in<G>().rt_outer)) return;
     // k, U and B lowered once: every invariant below is then a 4-term inner product
     R kd[4], Ud[4], Bd[4];
     symv(g, k, kd);
@@ -344,10 +356,16 @@ struct Ray {
     R C, S;
     if constexpr (kWP) {
       // the transported F1's components on (perp, para), from kappa at the point the state describes
-      wp_components(s.a, p0, k, perp, para, kappa, &C, &S);
+      if constexpr (sizeof(G) == sizeof(R)) {
+        wp_components(s.a, pg, k, perp, para, kappa, &C, &S);
+      } else {
+        const KerrPt<R> p0 = kerr_point_r(s.a, s.hs, rx, R(x0[2]));
+        wp_components(s.a, p0, k, perp, para, kappa, &C, &S);
+      }
     } else {
+      const R F[4] = {R(F0[0]), R(F0[1]), R(F0[2]), R(F0[3])};
       R pFd[4];
-      symv(g, F0, pFd);
+      symv(g, F, pFd);
       C = dot4(pFd, perp);
       S = dot4(pFd, para);
     }
@@ -355,6 +373,7 @@ struct Ray {
     const R c2 = (C * C - S * S) * inn, s2 = R(2) * C * S * inn;
     const R ratio = -kU;  // nu_plasma / nu_camera
     const SynchroSample<R> ss = synchro_sample(fl.theta_e, fl.n_e, fl.Bmag, sth, cth);
+    const R hlr = R(hl);
 #pragma unroll
     for (int f = 0; f < NF; f++) {
       if (f >= rc.nfreqs) break;
@@ -362,7 +381,7 @@ struct Ray {
       const Coeffs<R> cf = synchro_coeffs(ss, nu, rc.jscale[f]);
       R K[4][4], jv[4], E[4][4], Sg[4];
       build_K(cf, c2, s2, K, jv);
-      const R h = hl * rc.hconst[f];
+      const R h = hlr * rc.hconst[f];
       bool fp64 = false;
       if constexpr (kMixed) {
         const R kmax = fmax_t(fmax_t(fabs_t(cf.aI), fabs_t(cf.rV)), fabs_t(cf.rQ));

@@ -32,10 +32,11 @@ struct SnapView {
   R w0[3];  // base-level block widths
   R iw0up[3];  // finest-level slots per unit of x: 2^(nlevels-1) / w0
   R a, hs, gam;
-  // FP64 leaf geometry, used by the mixed-precision path to place FP32 samples in leaves and cells exactly
+  // FP64 leaf geometry and spacetime constants, used by the mixed-precision path (FP64 geodesic, FP32 plasma stage)
   const double* lbd;
   const double* dxcd;
   double xlo_d[4], xhi_d[4], w0_d[3];
+  double a_d, hs_d;
 
   PHX_HD SnapView<double, PT> fp64_view() const {
     SnapView<double, PT> v;
@@ -56,11 +57,13 @@ struct SnapView {
     v.nleafs = nleafs;
     v.nlevels = nlevels;
     v.cells = cells;
-    v.a = a;
-    v.hs = hs;
+    v.a = a_d;
+    v.hs = hs_d;
     v.gam = gam;
     v.lbd = lbd;
     v.dxcd = dxcd;
+    v.a_d = a_d;
+    v.hs_d = hs_d;
     return v;
   }
 };

@@ -34,6 +34,7 @@ struct PhxBatch {
   unsigned tile_mask = 0, trial_mask = 0;
   int32_t* jobs = nullptr;
   PhxFreqOut* out = nullptr;
+  PhxSpectrum* spec = nullptr;  // per-frequency totals of one item (phx_batch_spectrum)
   size_t nrecords = 0;
   unsigned long long* item_ctr = nullptr;
   unsigned long long* ctl = nullptr;
@@ -93,6 +94,7 @@ void build_items(PhxBatch* b, const PhxBatchItem* items, int32_t nitems, const s
     const PhxSnapshot* s = items[i].snapshot;
     h[i].rc = phx::make_consts<R>(b->params[i], s->a, s->hslope);
     h[i].snap = view_for<M, PT>(s);
+    h[i].snap_d = h[i].snap.fp64_view();
     h[i].jobs = b->jobs + job_off[i];
     h[i].out = reinterpret_cast<double*>(b->out + b->out_off[i]);
     h[i].pixstats = nullptr;
@@ -384,6 +386,20 @@ int phx_batch_device_result(PhxBatch* b, int32_t item, PhxFreqOut** d_res) {
     if (!b || !d_res) throw std::invalid_argument("null argument");
     if (item < 0 || item >= (int32_t)b->params.size()) throw std::invalid_argument("item out of range");
     *d_res = b->out + b->out_off[item];
+    return PHX_OK;
+  });
+}
+
+int phx_batch_spectrum(PhxBatch* b, int32_t item, PhxSpectrum* spec) {
+  return guarded([&]() -> int {
+    if (!b || !spec) throw std::invalid_argument("null argument");
+    if (item < 0 || item >= (int32_t)b->params.size()) throw std::invalid_argument("item out of range");
+    const PhxRenderParams& p = b->params[item];
+    if (!b->spec) b->spec = b->alloc<PhxSpectrum>(PHX_MAX_FREQS);
+    launch_spectrum(p, b->out + b->out_off[item], b->spec, b->stream);
+    ck(cudaMemcpyAsync(spec, b->spec, p.nfreqs * sizeof(PhxSpectrum), cudaMemcpyDeviceToHost, b->stream),
+       "D2H spectrum");
+    ck(cudaStreamSynchronize(b->stream), "spectrum");
     return PHX_OK;
   });
 }

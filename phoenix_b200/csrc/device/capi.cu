@@ -32,6 +32,7 @@ cudaError_t launch_mode(PhxSnapshot* s, const PhxRenderParams& p, const typename
   using R = typename phx::Policy<M>::R;
   phx::MarchArgs<R, PT> A;
   A.snap = snap_view<R, PT>(s, lb, dxc, prim);
+  A.snap_d = A.snap.fp64_view();
   A.rc = phx::make_consts<R>(p, s->a, s->hslope);
   A.jobs = d_jobs;
   A.njobs = njobs;
@@ -475,7 +476,8 @@ std::mutex g_noalloc_mutex;
 void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
 
 // Device address of the scratch array on the current device, resolved once per device (the symbol's host-side name
-// is only a stand-in and must never be passed to a kernel).
+// is only a stand-in and must never be passed to a kernel).  Kept until the process exits: a cudaDeviceReset would
+// unload the module and leave it stale, so the entry point is not for use across a device reset.
 void* noalloc_scratch(int device) {
   if (device < 0 || device >= kNoAllocMaxDevices) throw std::invalid_argument("device ordinal out of range");
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);

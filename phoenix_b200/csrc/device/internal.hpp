@@ -48,6 +48,9 @@ T* dev_upload(const T* host, size_t n, std::vector<void*>& owned) {
   return d;
 }
 
+// Launches the per-frequency image reduction (spectrum.cu) of a device-resident result.
+void launch_spectrum(const PhxRenderParams& p, const PhxFreqOut* d_res, PhxSpectrum* d_spec, cudaStream_t st);
+
 // Device workspace of the synchronous render entry (grown on demand, reused across calls).
 struct Workspace {
   int32_t* jobs = nullptr;
@@ -121,6 +124,8 @@ phx::SnapView<R, PT> snap_view(const PhxSnapshot* s, const R* lb, const R* dxc, 
   v.gam = R(s->gam);
   v.lbd = s->lb_d;
   v.dxcd = s->dxc_d;
+  v.a_d = s->a;
+  v.hs_d = s->hslope;
   for (int d = 0; d < 3; d++) {
     v.xlo_d[1 + d] = s->x_lo[d];
     v.xhi_d[1 + d] = s->x_hi[d];

@@ -32,6 +32,7 @@ enum CounterSlot {
 template <class R, class PT>
 struct MarchArgs {
   SnapView<R, PT> snap;
+  SnapView<double, PT> snap_d;  // FP64 leaf geometry and constants (the mixed mode's geodesic)
   RenderConsts<R> rc;
   const int32_t* jobs;
   int64_t njobs;
@@ -71,7 +72,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
             const int32_t pix = A.jobs[job];
             // a job outside the image is skipped, never written (the host checks job lists it uploads itself)
             if (pix >= 0 && pix < A.rc.W * A.rc.H) {
-              ray.init(A.snap, A.rc, pix);
+              ray.init(A.snap, A.snap_d, A.rc, pix);
               live = true;
             }
           }
@@ -81,7 +82,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
     if (!__any_sync(0xffffffffu, live)) break;
     for (int it = 0; it < A.period; it++) {
       if (live) {
-        live = ray.advance(A.snap, A.rc, ctr);
+        live = ray.advance(A.snap, A.snap_d, A.rc, ctr);
         if (!live) {
           ray.write(A.out, A.rc.nfreqs);
           if (A.pixstats) {

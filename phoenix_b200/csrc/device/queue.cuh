@@ -50,6 +50,7 @@ template <class R, class PT>
 struct alignas(128) ItemDesc {
   RenderConsts<R> rc;
   SnapView<R, PT> snap;
+  SnapView<double, PT> snap_d;   // FP64 leaf geometry and constants (the mixed mode's geodesic)
   const int32_t* jobs;
   double* out;                   // FreqOut records of the image
   int32_t* pixstats;             // optional per-pixel (steps, segments, bad)
@@ -120,7 +121,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
         d = A.items + raw.x;
         const int32_t pix = d->jobs[raw.y + off];
         if (pix >= 0 && pix < d->rc.W * d->rc.H) {
-          ray.init(d->snap, d->rc, pix);
+          ray.init(d->snap, d->snap_d, d->rc, pix);
           live = true;
         }
       }
@@ -145,7 +146,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
     idle = 0;
     for (int it = 0; it < A.period; it++) {
       if (live) {
-        live = ray.advance(d->snap, d->rc, ctr);
+        live = ray.advance(d->snap, d->snap_d, d->rc, ctr);
         if (!live) {
           ray.write(d->out, d->rc.nfreqs);
           if (d->pixstats) {

@@ -95,6 +95,7 @@ struct Request {
   size_t out_off = 0, out_bytes = 0;
   int64_t rays = 0;
   int64_t ntiles = 0, next_tile = 0;  // tiles of the request, and the first one not yet published
+  int retries = 0;                     // times it went back to the queue after the kernel ended early
   std::vector<PhxFreqOut> host;
   PhxRequestTiming t{};
   Clock::time_point submitted;
@@ -159,7 +160,9 @@ struct PhxServer {
   void stop_kernel();
   void reap();
   void fail_inflight(const std::string& why);
+  void requeue_inflight();
   void publish();
+  void ensure_kernel();
   void reset_queue();
 };
 
@@ -177,6 +180,7 @@ void bind_mode(PhxServer* s) {
     const PhxSnapshot* sn = self->snaps[r.snap];
     it.rc = phx::make_consts<R>(r.p, sn->a, sn->hslope);
     it.snap = view_for<M, PT>(sn);
+    it.snap_d = it.snap.fp64_view();
     it.jobs = jobs;
     it.out = reinterpret_cast<double*>(self->arena + r.out_off);
     it.pixstats = nullptr;
@@ -235,6 +239,8 @@ void PhxServer::start_generation() {
   std::fill(slot_req.begin(), slot_req.end(), 0);
 }
 
+// Stops the running kernel (called with nothing in flight).  A kernel that already left by its bounded idle wait
+// (status word set) is not an error here: no request was lost, and the next admission starts a new generation.
 void PhxServer::stop_kernel() {
   if (!kernel_running) return;
   unsigned long long* one = reinterpret_cast<unsigned long long*>(staging);
@@ -245,7 +251,10 @@ void PhxServer::stop_kernel() {
   kernel_running = false;
   unsigned long long status = 0;
   ck(cudaMemcpy(&status, ctl + phx::kQStatus, sizeof status, cudaMemcpyDeviceToHost), "status word");
-  if (status) throw std::runtime_error("the queue kernel gave up waiting for work (status word set)");
+  if (status) {
+    std::lock_guard<std::mutex> lk(mu);
+    stats.idle_exits++;
+  }
 }
 
 // Admits request r if its footprint fits and the generation has room; publishes it into the queue.
@@ -290,13 +299,17 @@ bool PhxServer::admit_one(Request& r) {
     r.t.admitted_s = seconds_since(r.submitted);
     inflight++;
   }
-  if (!kernel_running) {
-    ck(launch(compute, &lshape), "queue kernel launch");
-    ck(cudaEventRecord(kernel_done, compute), "event");
-    kernel_running = true;
-    generations++;
-  }
   return true;
+}
+
+// Starts the generation's kernel once it has published work: a kernel launched onto an empty queue would spend its
+// bounded idle wait before the first tiles arrive.
+void PhxServer::ensure_kernel() {
+  if (kernel_running || tiles_published == 0) return;
+  ck(launch(compute, &lshape), "queue kernel launch");
+  ck(cudaEventRecord(kernel_done, compute), "event");
+  kernel_running = true;
+  generations++;
 }
 
 // Publishes tiles of the admitted requests.  Small requests (at most small_rays rays) go in whole as soon as they are
@@ -311,7 +324,8 @@ void PhxServer::publish() {
   const long long slots = (long long)tiles_published * o.tile_rays;
   long long backlog = slots - (long long)*head_host;  // idle lanes' claims can pass the tail: then nothing is left
   if (backlog < 0) backlog = 0;
-  const long long lanes = (long long)std::max(lshape.grid, 1) * std::max(lshape.block, 128);
+  // resident lanes of the running kernel (before the generation's first launch: a whole-SM block of 512 per SM)
+  const long long lanes = lshape.grid > 0 ? (long long)lshape.grid * lshape.block : (long long)sms * 512;
   const long long limit = o.backlog_rays > 0 ? o.backlog_rays : 2 * lanes;
   phx::TileDesc* td = reinterpret_cast<phx::TileDesc*>(staging + ((item_bytes + 255) & ~(size_t)255));
   int64_t n = 0;
@@ -409,6 +423,36 @@ void PhxServer::fail_inflight(const std::string& why) {
   cv_done.notify_all();
 }
 
+// The kernel left by its bounded idle wait while requests were in flight (idle warps give up after idle_limit polls;
+// one that gave up holding a claim past the tail leaves that slot unserved).  Their results are incomplete: each goes
+// back to the front of the queue, in admission order, to be rendered again from scratch in a new generation (every
+// pixel is written once per run), at most kMaxRetries times before it fails.
+void PhxServer::requeue_inflight() {
+  constexpr int kMaxRetries = 2;
+  std::lock_guard<std::mutex> lk(mu);
+  std::vector<int64_t> back;
+  for (int32_t sl = 0; sl < next_slot; sl++) {
+    const int64_t id = slot_req[sl];
+    if (!id) continue;
+    Request* r = reqs.at(id).get();
+    alloc->release(r->out_off, r->out_bytes);
+    slot_req[sl] = 0;
+    inflight--;
+    if (r->retries < kMaxRetries) {
+      r->retries++;
+      r->state = PHX_REQ_QUEUED;
+      stats.retries++;
+      back.push_back(id);
+    } else {
+      r->state = PHX_REQ_FAILED;
+      r->error = "the queue kernel kept leaving before finishing the request (idle limit reached)";
+    }
+  }
+  pending.insert(pending.begin(), back.begin(), back.end());
+  reset_queue();
+  cv_done.notify_all();
+}
+
 void PhxServer::tick() {
   reap();
   if (kernel_running && cudaEventQuery(kernel_done) == cudaSuccess) {
@@ -418,9 +462,10 @@ void PhxServer::tick() {
     {
       std::lock_guard<std::mutex> lk(mu);
       any = inflight > 0;
+      stats.idle_exits++;
     }
     reap();
-    if (any) fail_inflight("the queue kernel left before finishing its requests (idle limit reached)");
+    if (any) requeue_inflight();
     reset_queue();
   }
   const bool fresh = !kernel_running && next_slot == 0 && tiles_reserved == 0;
@@ -441,6 +486,7 @@ void PhxServer::tick() {
     pending.pop_front();
   }
   publish();
+  ensure_kernel();
   int64_t nin;
   bool has_pending;
   {

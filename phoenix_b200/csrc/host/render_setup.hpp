@@ -40,6 +40,21 @@ inline void check_params(const PhxRenderParams& p) {
   if (p.precision < PHX_PREC_FP32 || p.precision > PHX_PREC_MIXED) bad("unknown precision mode");
 }
 
+// Integration limits and step-size constants of a geodesic in precision G (the reference's FP32 / FP64 thresholds,
+// core/numerics/precision.hpp:51-56).
+template <class G>
+StepConsts<G> step_consts(const PhxRenderParams& p, double r_h) {
+  StepConsts<G> c;
+  c.stepsize = G(p.stepsize);
+  c.inv_stepsize = G(1.0 / p.stepsize);
+  c.cut_in = G(r_h * (1.0 + p.horizon_margin));
+  c.r_out = G(1.1 * p.r_cam);
+  c.rt_outer = G(p.rt_outer);
+  c.tiny = sizeof(G) == 4 ? G(1e-30) : G(1e-160);
+  c.big = sizeof(G) == 4 ? G(1e30) : G(1e100);
+  return c;
+}
+
 template <class R>
 RenderConsts<R> make_consts(const PhxRenderParams& p, double a, double hslope) {
   RenderConsts<R> rc;
@@ -53,21 +68,17 @@ RenderConsts<R> make_consts(const PhxRenderParams& p, double a, double hslope) {
   rc.fov_y = p.fov_y;
   rc.cos_pa = std::cos(p.pa / 180.0 * kPi);
   rc.sin_pa = std::sin(p.pa / 180.0 * kPi);
-  rc.cam.a = (double)R(a);
-  rc.cam.hslope = (double)R(hslope);
+  // the camera set-up sees the spin and hslope in the geodesic's precision (FP64 for FP64 and mixed renders)
+  const bool geo64 = sizeof(R) == 8 || p.precision == PHX_PREC_MIXED;
+  rc.cam.a = geo64 ? a : (double)R(a);
+  rc.cam.hslope = geo64 ? hslope : (double)R(hslope);
   rc.cam.incl_deg = p.inclination;
   rc.cam.phi_deg = p.phi;
   rc.cam.r_cam = p.r_cam;
   rc.cam.t_init = p.t_init;
-  rc.stepsize = R(p.stepsize);
-  rc.inv_stepsize = R(1.0 / p.stepsize);
   const double r_h = 1.0 + std::sqrt(1.0 - a * a);
-  rc.cut_in = R(r_h * (1.0 + p.horizon_margin));
-  rc.r_out = R(1.1 * p.r_cam);
-  rc.rt_outer = R(p.rt_outer);
-  rc.step_tiny = sizeof(R) == 4 ? R(1e-30) : R(1e-160);
-  rc.step_big = sizeof(R) == 4 ? R(1e30) : R(1e100);
-  rc.r_fp64 = R((p.r_fp64 > 0.0 ? p.r_fp64 : 3.0) * r_h);
+  rc.step = step_consts<R>(p, r_h);
+  rc.step_d = step_consts<double>(p, r_h);
   rc.tau_fp64 = R(p.tau_fp64 > 0.0 ? p.tau_fp64 : 0.1);
   rc.pv.Ne = R(u.Ne);
   rc.pv.Bu = R(u.B);

@@ -31,13 +31,19 @@ EXPORTS = ["phx_default_params", "phx_snapshot_create", "phx_snapshot_load", "ph
            "phx_batch_result", "phx_batch_device_result", "phx_batch_tuning", "phx_batch_destroy",
            "phx_default_server_options", "phx_server_create", "phx_server_submit", "phx_server_poll",
            "phx_server_wait", "phx_server_result", "phx_server_stats", "phx_server_destroy",
-           "phx_snapshot_info", "phx_snapshot_download"]
+           "phx_snapshot_info", "phx_snapshot_download", "phx_spectrum_async", "phx_batch_spectrum",
+           "phx_measure_fp32_peak"]
 REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
 TUNE_MAX_CANDIDATES = 16
 
 
 class PhxFreqOut(C.Structure):
     _fields_ = [("IQUV", C.c_double * 4), ("tau", C.c_double), ("tauF", C.c_double)]
+
+
+class PhxSpectrum(C.Structure):
+    _fields_ = [("IQUV", C.c_double * 4), ("tau_mean", C.c_double), ("tauF_mean", C.c_double),
+                ("n_flux", C.c_int64), ("n_tau", C.c_int64)]
 
 
 class PhxSnapshotDesc(C.Structure):
@@ -144,7 +150,8 @@ class PhxRequestTiming(C.Structure):
 class PhxServerStats(C.Structure):
     _fields_ = [(n, C.c_int64) for n in ("submitted", "completed", "inflight", "pending", "generations", "rays",
                                          "steps", "snapshot_bytes", "table_bytes", "arena_bytes", "arena_used",
-                                         "job_table_bytes")] + [("grid", C.c_int32), ("regs", C.c_int32)]
+                                         "job_table_bytes")] + [("grid", C.c_int32), ("regs", C.c_int32),
+                                                                ("idle_exits", C.c_int64), ("retries", C.c_int64)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -197,6 +204,9 @@ def lib():
     L.phx_batch_result.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, P(PhxRenderInfo)]
     L.phx_batch_device_result.argtypes = [C.c_void_p, C.c_int32, P(C.c_void_p)]
     L.phx_batch_tuning.argtypes = [C.c_void_p, P(PhxBatchTuning)]
+    L.phx_batch_spectrum.argtypes = [C.c_void_p, C.c_int32, P(PhxSpectrum)]
+    L.phx_spectrum_async.argtypes = [P(PhxRenderParams), C.c_void_p, C.c_void_p, C.c_void_p]
+    L.phx_measure_fp32_peak.argtypes = [C.c_int32, P(C.c_double)]
     L.phx_batch_destroy.argtypes = [C.c_void_p]
     L.phx_batch_destroy.restype = None
     L.phx_snapshot_info.argtypes = [C.c_void_p, P(PhxSnapshotInfo)]
@@ -218,7 +228,8 @@ def lib():
         getattr(L, name).restype = C.c_int
     for name in ("phx_snapshot_create", "phx_snapshot_load", "phx_bhac_read", "phx_bhac_describe", "phx_schedule_morton",
                  "phx_render", "phx_render_async", "phx_render_noalloc", "phx_batch_create", "phx_batch_launch",
-                 "phx_batch_run", "phx_batch_result", "phx_batch_device_result", "phx_batch_tuning"):
+                 "phx_batch_run", "phx_batch_result", "phx_batch_device_result", "phx_batch_tuning",
+                 "phx_batch_spectrum", "phx_spectrum_async", "phx_measure_fp32_peak"):
         getattr(L, name).restype = C.c_int
     _lib = L
     return L

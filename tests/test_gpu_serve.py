@@ -121,3 +121,46 @@ def test_small_request_overtakes_a_large_one(snaps):
     assert np.array_equal(rs, ra)
     single, _ = snaps[0].render(big_p)
     assert flux_errors(rb, single, big_p).max() <= 1e-5
+
+
+def test_idle_limit_exit_then_clean_relaunch(snaps):
+    """The queue kernel's idle wait is bounded: with a small idle_limit and a long linger, the kernel gives up on its
+    own after the first request (status word set, no request lost), and the next submission relaunches it in a new
+    generation with the same result."""
+    p = _params("edge", "fp32")
+    with P.Server(snaps, "fp32", max_freqs=1, idle_limit=200, idle_ns=1000, linger_ms=600000.0) as srv:
+        first = srv.submit(1, p)
+        srv.wait(first, WAIT)
+        a, _ = srv.result(first)
+        t0 = time.time()
+        while srv.stats()["idle_exits"] < 1 and time.time() - t0 < 30.0:
+            time.sleep(0.01)
+        st = srv.stats()
+        assert st["idle_exits"] >= 1 and st["inflight"] == 0
+        second = srv.submit(1, p)
+        srv.wait(second, WAIT)
+        b, _ = srv.result(second)
+        st = srv.stats()
+    assert st["generations"] >= 2 and st["completed"] == 2
+    assert np.array_equal(a, b)
+
+
+def test_requests_survive_kernel_idle_exits(snaps):
+    """An idle_limit of a few polls makes the kernel leave whenever the queue runs dry for a moment, also while other
+    requests are still in flight (a warp that gives up may hold a claim past the tail).  Requests caught by such an
+    exit go back to the queue and are rendered again; every result equals the request rendered alone."""
+    ps = [_params("edge", "fp32", inclination=150.0 + 5 * k) for k in range(6)]
+    with P.Server(snaps, "fp32", max_freqs=1, idle_limit=2, idle_ns=100, linger_ms=600000.0) as srv:
+        ids = []
+        for p in ps:
+            ids.append(srv.submit(1, p))
+            time.sleep(0.002)
+        got = []
+        for rid in ids:
+            srv.wait(rid, WAIT)
+            got.append(srv.result(rid)[0])
+        st = srv.stats()
+    assert st["completed"] == len(ps) and st["idle_exits"] >= 1
+    for p, r in zip(ps, got):
+        single, _ = snaps[1].render(p)
+        assert flux_errors(r, single, p).max() <= 1e-5
