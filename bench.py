@@ -36,8 +36,10 @@ WORKLOAD = dict(base=(192, 96, 96), nlevels=3, refine=(3.5, 25.0, 0.55), seed=0,
                 inclinations=(10.0, 60.0, 163.0), frequency=230e9, m_unit=1.2e18)
 # Algorithmic FP32 flops per unit of work: per ray-step (RK4 with four metric/Christoffel evaluations, step size),
 # per emitting sample (metric, fluid, tetrad, pitch angle), per (sample, frequency) (coefficients, segment operator,
-# accumulation).  Op-count estimates of the reference path, frozen here so that every run uses the same figures.
-FLOPS = dict(step=1800.0, sample=900.0, freq=850.0)
+# accumulation).  Counted in the reference's own FP32 code with an op-counting scalar and fitted over pixel samples of
+# this workload (oracle/opcount/count_flops.py --workload plain: 3445.2 / 869.7 / 1223.6, fit residual 0.4%; add,
+# sub, mul 1 flop; div, sqrt 4; exp, log 8; sin, cos 10; other transcendentals 10-20), frozen here.
+FLOPS = dict(step=3445.0, sample=870.0, freq=1224.0)
 # Algorithmic bytes the march requests from the memory system: per emitting sample the 8 corners x 8 FP32 primitives
 # of the trilinear gather (256 B); per step the flattened leaf-map entry (4 B) and the leaf's lb/dxc (24 B); per ray
 # its job index (4 B) and one 48 B FreqOut record per frequency.
@@ -840,8 +842,8 @@ def main():
                          "launch_ms": kavg_s * 1e3, "flops_per_launch": flops / nlaunch,
                          "flops_per_unit": FLOPS, "fma_pipe_active": FMA_PIPE_ACTIVE,
                          "note": "the march is bound by FP32 instruction issue: algorithmic FP32 flops per launch "
-                                 "(per ray-step, per emitting sample, per sample-frequency) over the CUDA-event launch "
-                                 "time; peak = FP32 FMA issue rate measured on this GPU in this run "
+                                 "(per ray-step, per emitting sample, per sample-frequency, counted in the reference's "
+                                 "own FP32 code) over the CUDA-event launch time; peak = FP32 FMA issue rate measured on this GPU in this run "
                                  "(phx_measure_fp32_peak); traffic = DRAM bytes per launch; fma_pipe_active = the "
                                  "FMA-pipe share of cycles from ncu on this workload"},
             "roofline_hbm": {"bound": "hbm", "achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s",
