@@ -228,10 +228,16 @@ typedef struct {
   int32_t blocks_per_sm;   /* register-cap variant (FP32: 1, 3, 4; mixed 1, 3), 0 = default (FP32 4, mixed 3, FP64 1) or autotuned */
   int32_t period;          /* march passes between lane refills, 0 = default 64 or autotuned */
   int32_t autotune;        /* nonzero: time every (blocks_per_sm, period) candidate on a sample of the batch's tiles
-                              at creation and keep the fastest */
+                              at creation, then every tile shape at the fastest of them, and keep the fastest */
   int32_t sample_stride;   /* autotune sample: every n-th tile, 0 = 16 */
   int32_t keep_order;      /* nonzero: tiles in item order; 0: the largest images' tiles first */
+  int32_t tile_shape;      /* pixel order of the items without a job list, i.e. the shape of the pixel tile a warp's
+                              32 consecutive rays cover: PHX_TILE_* (0 = Morton, the reference's schedule) */
 } PhxBatchOptions;
+
+/* Tile shapes: Morton (Z-order, 8x4-pixel warp tiles, the reference's host::jobs::schedule), or tiles of w x h pixels
+ * (pixels j-fastest inside a tile, tiles in Morton order of their coordinates). */
+enum { PHX_TILE_MORTON = 0, PHX_TILE_16X2 = 1, PHX_TILE_32X1 = 2, PHX_TILE_4X8 = 3, PHX_TILE_SHAPES = 4 };
 
 #define PHX_TUNE_MAX_CANDIDATES 16
 typedef struct {
@@ -240,6 +246,8 @@ typedef struct {
   int32_t ncand;  /* candidates timed by the autotuner (0 if it did not run) */
   int32_t cand_blocks_per_sm[PHX_TUNE_MAX_CANDIDATES], cand_period[PHX_TUNE_MAX_CANDIDATES];
   double cand_ms[PHX_TUNE_MAX_CANDIDATES];
+  int32_t tile_shape;  /* PHX_TILE_* in use */
+  int32_t cand_tile_shape[PHX_TUNE_MAX_CANDIDATES];
   int64_t nitems, ntiles, nrays;
   int64_t device_bytes;  /* device memory the batch holds (tables, job lists, results) */
 } PhxBatchTuning;
@@ -298,7 +306,7 @@ typedef struct {
   double linger_ms;       /* idle time after which the scheduler stops the kernel, default 20 */
   int32_t poll_us;        /* scheduler polling interval, default 50 */
   int32_t publish_chunk;  /* tiles a large request publishes at a time, default 64 */
-  int64_t backlog_rays;   /* published but unclaimed rays kept in the queue, 0 = two grid-loads of lanes */
+  int64_t backlog_rays;   /* published but unclaimed rays kept in the queue, 0 = half a grid-load of lanes */
   int64_t small_rays;     /* requests of at most this many rays enter the queue whole, ahead of the large ones'
                              remaining tiles (default 65536, a 256^2 image) */
 } PhxServerOptions;

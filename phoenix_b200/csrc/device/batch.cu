@@ -27,6 +27,9 @@ struct PhxBatch {
   std::vector<PhxRenderParams> params;
   std::vector<int64_t> njobs;
   std::vector<size_t> out_off;  // record offsets into out
+  std::vector<size_t> job_off;  // job-list offsets into jobs
+  std::vector<char> own_order;  // item's job list is the batch's pixel order (no caller job list)
+  int tile_shape = PHX_TILE_MORTON;
   void* items = nullptr;
   phx::TileDesc* tiles = nullptr;
   phx::TileDesc* trial = nullptr;
@@ -75,6 +78,38 @@ struct PhxBatch {
 };
 
 namespace {
+
+// Pixel order of a W x H image for a tile shape (PHX_TILE_*): Morton, or w x h tiles (j fastest inside a tile) in
+// Morton order of the tile coordinates.
+std::vector<int32_t> pixel_order(int32_t W, int32_t H, int shape) {
+  std::vector<int32_t> m((size_t)W * H);
+  if (shape == PHX_TILE_MORTON) {
+    if (phx_schedule_morton(W, H, m.data()) != PHX_OK) throw std::runtime_error(last_error());
+    return m;
+  }
+  static const int dims[PHX_TILE_SHAPES][2] = {{8, 4}, {16, 2}, {32, 1}, {4, 8}};
+  const int tw = dims[shape][0], th = dims[shape][1];
+  const int32_t nti = (W + tw - 1) / tw, ntj = (H + th - 1) / th;
+  std::vector<int32_t> tiles((size_t)nti * ntj);
+  if (phx_schedule_morton(nti, ntj, tiles.data()) != PHX_OK) throw std::runtime_error(last_error());
+  size_t n = 0;
+  for (const int32_t t : tiles) {
+    const int32_t ti = t / ntj, tj = t % ntj;
+    for (int32_t i = ti * tw; i < std::min(W, (ti + 1) * tw); i++)
+      for (int32_t j = tj * th; j < std::min(H, (tj + 1) * th); j++) m[n++] = i * H + j;
+  }
+  return m;
+}
+
+// Writes every own-order item's job list for `shape` into the device job array.
+void upload_order(PhxBatch* b, int shape) {
+  for (size_t i = 0; i < b->params.size(); i++) {
+    if (!b->own_order[i]) continue;
+    const std::vector<int32_t> m = pixel_order(b->params[i].img_width, b->params[i].img_height, shape);
+    ck(cudaMemcpy(b->jobs + b->job_off[i], m.data(), m.size() * sizeof(int32_t), cudaMemcpyHostToDevice), "H2D jobs");
+  }
+  b->tile_shape = shape;
+}
 
 unsigned pow2_mask(int64_t n) {
   unsigned long long c = 1;
@@ -155,18 +190,43 @@ void autotune(PhxBatch* b) {
   // load every variant once (an empty queue: the kernel leaves at its first refill)
   phx::LaunchShape ls;
   for (const auto& q : cand) timed_launch(b, b->trial, 0, b->trial_mask, 1, q, &ls);
-  b->tuning.ncand = (int32_t)cand.size();
+  int nc = 0;
+  auto record = [&](const phx::QueueShape& q, int shape, float ms) {
+    if (nc >= PHX_TUNE_MAX_CANDIDATES) return;
+    b->tuning.cand_blocks_per_sm[nc] = q.blocks_per_sm;
+    b->tuning.cand_period[nc] = q.period;
+    b->tuning.cand_tile_shape[nc] = shape;
+    b->tuning.cand_ms[nc] = ms;
+    nc++;
+  };
+  // stage 1: register cap x refill period, in the current pixel order
+  const int shape0 = b->tile_shape;
   float best = 1e30f;
   for (size_t c = 0; c < cand.size(); c++) {
     const float ms = timed_launch(b, b->trial, b->ntrial, b->trial_mask, b->trial_rays, cand[c], &ls);
-    b->tuning.cand_blocks_per_sm[c] = cand[c].blocks_per_sm;
-    b->tuning.cand_period[c] = cand[c].period;
-    b->tuning.cand_ms[c] = ms;
+    record(cand[c], shape0, ms);
     if (ms < best) {
       best = ms;
       b->shape = cand[c];
     }
   }
+  // stage 2: the other tile shapes at the best launch shape (only items without a caller job list change order)
+  const bool any_own = std::any_of(b->own_order.begin(), b->own_order.end(), [](char c) { return c != 0; });
+  int best_shape = shape0;
+  if (any_own) {
+    for (int shape = 0; shape < PHX_TILE_SHAPES; shape++) {
+      if (shape == shape0) continue;
+      upload_order(b, shape);
+      const float ms = timed_launch(b, b->trial, b->ntrial, b->trial_mask, b->trial_rays, b->shape, &ls);
+      record(b->shape, shape, ms);
+      if (ms < best) {
+        best = ms;
+        best_shape = shape;
+      }
+    }
+    if (b->tile_shape != best_shape) upload_order(b, best_shape);
+  }
+  b->tuning.ncand = nc;
 }
 
 void capture(PhxBatch* b) {
@@ -211,8 +271,12 @@ PhxBatch* create_batch(const PhxBatchItem* items, int32_t nitems, const PhxBatch
   if (b->nf_slots > 4 && b->precision != PHX_PREC_FP32)
     throw std::invalid_argument("batches with more than 4 frequencies per image are FP32 only");
   // job lists (validated) and result offsets
+  if (o.tile_shape < 0 || o.tile_shape >= PHX_TILE_SHAPES) throw std::invalid_argument("unknown tile_shape");
+  b->tile_shape = o.tile_shape;
   std::vector<int32_t> all_jobs;
-  std::vector<size_t> job_off(nitems);
+  std::vector<size_t>& job_off = b->job_off;
+  job_off.assign(nitems, 0);
+  b->own_order.assign(nitems, 0);
   b->params.resize(nitems);
   b->njobs.resize(nitems);
   b->out_off.resize(nitems);
@@ -231,10 +295,10 @@ PhxBatch* create_batch(const PhxBatchItem* items, int32_t nitems, const PhxBatch
       }
       b->njobs[i] = items[i].njobs;
     } else {
-      std::vector<int32_t> m((size_t)npix);
-      if (phx_schedule_morton(p.img_width, p.img_height, m.data()) != PHX_OK) throw std::runtime_error(last_error());
+      const std::vector<int32_t> m = pixel_order(p.img_width, p.img_height, b->tile_shape);
       all_jobs.insert(all_jobs.end(), m.begin(), m.end());
       b->njobs[i] = npix;
+      b->own_order[i] = 1;
     }
     nrec = (nrec + 3) & ~(size_t)3;  // 192-byte aligned records per item
     b->out_off[i] = nrec;
@@ -300,6 +364,7 @@ PhxBatch* create_batch(const PhxBatchItem* items, int32_t nitems, const PhxBatch
   b->tuning.blocks_per_sm = b->shape.blocks_per_sm;
   b->tuning.period = b->shape.period;
   b->tuning.tile_rays = b->tile_rays;
+  b->tuning.tile_shape = b->tile_shape;
   b->tuning.grid = b->lshape.grid;
   b->tuning.block = b->lshape.block;
   b->tuning.regs = b->lshape.regs;

@@ -314,9 +314,11 @@ void PhxServer::ensure_kernel() {
 
 // Publishes tiles of the admitted requests.  Small requests (at most small_rays rays) go in whole as soon as they are
 // admitted; large ones go in first in, first out, a chunk at a time while the queue's backlog of published but
-// unclaimed rays is below about two grid-loads of lanes.  A small request that arrives behind a large one therefore
-// waits for that backlog, not for every ray of the large one, while the large ones keep their order and their rays'
-// coherence (interleaving them all round robin mixes snapshots and images in the caches and costs throughput).
+// unclaimed rays is below half a grid-load of lanes (about 20 ms of work on a B200: far more than one scheduler tick
+// needs to top it up, and little for a later request to wait behind).  A small request that arrives behind a large
+// one therefore waits for that backlog, not for every ray of the large one, while the large ones keep their order and
+// their rays' coherence (interleaving them all round robin mixes snapshots and images in the caches and costs
+// throughput).
 void PhxServer::publish() {
   if (unpublished.empty()) return;
   ck(cudaMemcpyAsync(head_host, ctl + phx::kQHead, sizeof *head_host, cudaMemcpyDeviceToHost, copy), "D2H head");
@@ -326,7 +328,7 @@ void PhxServer::publish() {
   if (backlog < 0) backlog = 0;
   // resident lanes of the running kernel (before the generation's first launch: a whole-SM block of 512 per SM)
   const long long lanes = lshape.grid > 0 ? (long long)lshape.grid * lshape.block : (long long)sms * 512;
-  const long long limit = o.backlog_rays > 0 ? o.backlog_rays : 2 * lanes;
+  const long long limit = o.backlog_rays > 0 ? o.backlog_rays : lanes / 2;
   phx::TileDesc* td = reinterpret_cast<phx::TileDesc*>(staging + ((item_bytes + 255) & ~(size_t)255));
   int64_t n = 0;
   auto put = [&](Request* r, int64_t m) {

@@ -95,7 +95,8 @@ class PhxBatchItem(C.Structure):
 
 class PhxBatchOptions(C.Structure):
     _fields_ = [("tile_rays", C.c_int32), ("blocks_per_sm", C.c_int32), ("period", C.c_int32),
-                ("autotune", C.c_int32), ("sample_stride", C.c_int32), ("keep_order", C.c_int32)]
+                ("autotune", C.c_int32), ("sample_stride", C.c_int32), ("keep_order", C.c_int32),
+                ("tile_shape", C.c_int32)]
 
 
 class PhxBatchTuning(C.Structure):
@@ -104,6 +105,7 @@ class PhxBatchTuning(C.Structure):
         ("grid", C.c_int32), ("block", C.c_int32), ("regs", C.c_int32), ("local_bytes", C.c_int32),
         ("ncand", C.c_int32), ("cand_blocks_per_sm", C.c_int32 * TUNE_MAX_CANDIDATES),
         ("cand_period", C.c_int32 * TUNE_MAX_CANDIDATES), ("cand_ms", C.c_double * TUNE_MAX_CANDIDATES),
+        ("tile_shape", C.c_int32), ("cand_tile_shape", C.c_int32 * TUNE_MAX_CANDIDATES),
         ("nitems", C.c_int64), ("ntiles", C.c_int64), ("nrays", C.c_int64), ("device_bytes", C.c_int64),
     ]
 
@@ -111,7 +113,7 @@ class PhxBatchTuning(C.Structure):
         n = self.ncand
         d = {name: getattr(self, name) for name, _ in self._fields_ if not name.startswith("cand_")}
         d["candidates"] = [dict(blocks_per_sm=self.cand_blocks_per_sm[i], period=self.cand_period[i],
-                                ms=self.cand_ms[i]) for i in range(n)]
+                                tile_shape=self.cand_tile_shape[i], ms=self.cand_ms[i]) for i in range(n)]
         return d
 
 

@@ -12,10 +12,8 @@ import sys
 
 import pytest
 
+from oracle import build_ref
 from tests.conftest import ROOT
-
-sys.path.insert(0, os.path.join(ROOT, "oracle"))
-import build_ref  # noqa: E402
 
 
 @pytest.mark.skipif(not os.path.isdir(os.path.join(build_ref.default_src(), "src")),
