@@ -39,6 +39,10 @@ DEVICE_SRC = ["device/march_fp64_f64.cu", "device/march_fp64_f32.cu", "device/ma
               "device/queue_dispatch.cu", "device/batch.cu", "device/server.cu",
               "device/decode.cu", "device/spectrum.cu", "device/peak.cu"]
 HOST_SRC = ["host/snapshot.cpp", "host/output.cpp", "host/hdf5_writer.cpp"]
+# The FP64 kernels follow the reference's FP64 CPU arithmetic, which rounds every product and sum separately: no
+# multiply-add contraction there (explicit fma() calls stay fused).
+NVCC_FILE_FLAGS = {src: ["-fmad=false"] for src in ("device/march_fp64_f64.cu", "device/march_fp64_f32.cu",
+                                                     "device/queue_fp64.cu")}
 CLI_SRC = ["host/main.cpp", "host/config.cpp"]
 
 
@@ -82,7 +86,7 @@ def build(jobs: int = 0, force: bool = False, verbose: bool = False) -> dict:
         objs.append(obj)
         if force or _stale(obj, [path] + headers):
             if src.endswith(".cu"):
-                cmd = ["nvcc"] + NVCC_FLAGS + ["-I" + INCLUDE, "-c", path, "-o", obj]
+                cmd = ["nvcc"] + NVCC_FLAGS + NVCC_FILE_FLAGS.get(src, []) + ["-I" + INCLUDE, "-c", path, "-o", obj]
             else:
                 cmd = ["g++"] + CXX_FLAGS + ["-I" + INCLUDE, "-c", path, "-o", obj]
             tasks.append((cmd, obj + ".log"))

@@ -159,6 +159,22 @@ inline float rsqrt(float x) { return 1.0f / std::sqrt(x); }
 inline float tanh(float x) { return std::tanh(x); }
 inline float cos(float x) { return std::cos(x); }
 #endif
+// 1/x for the FP64 geodesic of the mixed mode: a single-precision reciprocal refined by two Newton-Raphson steps
+// r <- r + r (1 - x r) in FP64 (each squares the relative error: ~1e-7 -> ~1e-14 -> rounding), about 1 ulp and fewer
+// instructions than an IEEE division.  Arguments outside float's normal range take the division.
+PHX_HD double rcp_nr(double x) {
+  const double ax = x < 0.0 ? -x : x;
+  if (!(ax > 1e-30 && ax < 1e30)) return 1.0 / x;
+#if defined(__CUDA_ARCH__)
+  double r = (double)__fdividef(1.0f, (float)x);
+#else
+  double r = (double)(1.0f / (float)x);
+#endif
+  double e = fma(-x, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-x, r, 1.0);
+  return fma(r, e, r);
+}
 PHX_HD double exp(double x) { return exp_t(x); }
 PHX_HD double log(double x) { return log_t(x); }
 PHX_HD double div(double a, double b) { return a / b; }

@@ -72,9 +72,10 @@ PHX_HD T exp_small(T d) {
 // ((d0 + d3) + 2 (d1 + d2)) dt/6 needs two 12-vectors instead of four.  The stage loop is deliberately not unrolled:
 // one copy of the stage body (metric, derivatives, both Christoffel contractions) keeps the march loop small enough
 // for the instruction cache, which four unrolled copies overflow.
-// kShift (uncompensated state only): each stage's exp(x1) and sincos(x2) come from the step's starting point and short
-// series of the stage offset (exp_small, sincos_small: exact to rounding for the offsets allowed), one exp and one
-// sincos per step instead of four; a stage whose offset is larger evaluates the point directly.
+// kShift (uncompensated state only; the mixed mode's FP64 geodesic): each stage's exp(x1) and sincos(x2) come from the
+// step's starting point and short series of the stage offset (exp_small, sincos_small: exact to rounding for the
+// offsets allowed), one exp and one sincos per step instead of four, and the geometry's reciprocals are the
+// Newton-refined FP64 ones (fastm::rcp_nr); a stage whose offset is larger evaluates the point directly.
 template <class R, bool kComp, int NS, bool kShift = false>
 PHX_HD void rk4_step(R a, R hs, GeoState<R, NS>& g, R dt) {
   constexpr bool kF = NS == 12;
@@ -109,8 +110,9 @@ PHX_HD void rk4_step(R a, R hs, GeoState<R, NS>& g, R dt) {
       if (fabs_t(d1) <= R(0.1) && fabs_t(d2) <= R(0.5)) {
         R sd, cd;
         sincos_small(d2, &sd, &cd);
-        const KerrPt<R> p = kerr_point_rsc(a, hs, e0 * exp_small(d1), y[2], sx0 * cd + cx0 * sd, cx0 * cd - sx0 * sd);
-        geodesic_accel_at<R, kF>(a, p, y + 4, y + 8, d + 4, d + 8);
+        const KerrPt<R> p =
+            kerr_point_rsc<R, true>(a, hs, e0 * exp_small(d1), y[2], sx0 * cd + cx0 * sd, cx0 * cd - sx0 * sd);
+        geodesic_accel_at<R, kF, true>(a, p, y + 4, y + 8, d + 4, d + 8);
       } else {
         geodesic_accel<R, kF>(a, hs, y[1], y[2], y + 4, y + 8, d + 4, d + 8);
       }
@@ -198,15 +200,16 @@ PHX_HD R step_size(R stepsize, R x2, const R k[4], const R* dxc, R tiny, R big) 
 // The same rule with the reciprocals folded (FP32 paths): 1 / (stepsize / |k| + tiny) -> |k| / stepsize and
 // 1 / (dxc / |k| + tiny) -> |k| / dxc with the leaf's inverse cell sizes idxc, so that two divisions remain instead of
 // twelve.  Equal to step_size up to rounding; the pole term keeps the reference's 1 / tiny limit at x2 = 0.
-template <class R>
+// kNR: the mixed mode's FP64 reciprocals (geo_rcp, geo_div).
+template <class R, bool kNR = false>
 PHX_HD R step_size_fast(R stepsize, R inv_stepsize, R x2, const R k[4], const R* idxc, R tiny, R big) {
   const R a1 = fabs_t(k[1]) + tiny, a2 = fabs_t(k[2]) + tiny, a3 = fabs_t(k[3]) + tiny;
   const R m = fmin_t(x2, R(kPi) - x2);
-  const R i2 = fmin_t(fastm::div(a2, stepsize * m), R(1) / tiny);  // m = 0 (or underflow): the reference's 1 / tiny
+  const R i2 = fmin_t(geo_div<R, kNR>(a2, stepsize * m), R(1) / tiny);  // m = 0: the reference's 1 / tiny
   const R sum = (a1 + a3) * inv_stepsize + i2;
   R grid = big;
-  if (idxc) grid = fastm::div(R(0.25), a1 * idxc[0] + a2 * idxc[1] + a3 * idxc[2]);
-  return -fmin_t(fastm::rcp(sum), grid);
+  if (idxc) grid = geo_div<R, kNR>(R(0.25), a1 * idxc[0] + a2 * idxc[1] + a3 * idxc[2]);
+  return -fmin_t(geo_rcp<R, kNR>(sum), grid);
 }
 
 // Re-solve k^t from the spatial components so that g_{mu nu} k^mu k^nu = 0 (the larger root), as the reference

@@ -76,8 +76,28 @@ PHX_HD void sincos_small(T d, T* sn, T* cs) {
   *cs = c;
 }
 
+// Reciprocal and quotient of the geometry code: the type's fast form (FP32: hardware reciprocal; FP64: exact division),
+// or with kNR (the mixed mode's FP64 geodesic) the Newton-refined FP64 reciprocal.
+template <class T, bool kNR>
+PHX_HD T geo_rcp(T x) {
+  if constexpr (kNR && sizeof(T) == 8) {
+    return fastm::rcp_nr(x);
+  } else {
+    return fastm::rcp(x);
+  }
+}
+
+template <class T, bool kNR>
+PHX_HD T geo_div(T a, T b) {
+  if constexpr (kNR && sizeof(T) == 8) {
+    return a * fastm::rcp_nr(b);
+  } else {
+    return fastm::div(a, b);
+  }
+}
+
 // Geometry at (r, x2) when r = exp(x1) and sin x2, cos x2 are already known.
-template <class T>
+template <class T, bool kNR = false>
 PHX_HD KerrPt<T> kerr_point_rsc(T a, T hs, T r, T x2, T sx, T cx) {
   KerrPt<T> p;
   p.r = r;
@@ -97,7 +117,7 @@ PHX_HD KerrPt<T> kerr_point_rsc(T a, T hs, T r, T x2, T sx, T cx) {
   }
   p.s2 = p.s * p.s;
   p.sig = p.r * p.r + a * a * p.c * p.c;
-  p.isig = fastm::rcp(p.sig);  // FP32: hardware reciprocal (2 ulp), FP64: exact division
+  p.isig = geo_rcp<T, kNR>(p.sig);  // FP32: hardware reciprocal (2 ulp), FP64: exact division or Newton-refined
   p.q = T(2) * p.r * p.isig;
   return p;
 }
@@ -129,13 +149,13 @@ PHX_HD Cov<T> cov_metric(const KerrPt<T>& p, T a) {
   return g;
 }
 
-template <class T>
+template <class T, bool kNR = false>
 PHX_HD Contra<T> contra_metric(const KerrPt<T>& p, T a) {
   Contra<T> u;
   const T isig = p.isig;
-  const T ir = fastm::rcp(p.r);
+  const T ir = geo_rcp<T, kNR>(p.r);
   const T tp2 = p.tp * p.tp;
-  const T iprod = isig * fastm::rcp(tp2 * p.s2);  // one reciprocal for both 1 / theta'^2 and 1 / sin^2
+  const T iprod = isig * geo_rcp<T, kNR>(tp2 * p.s2);  // one reciprocal for both 1 / theta'^2 and 1 / sin^2
   u.tt = -(T(1) + p.q);
   u.t1 = T(2) * isig;
   u.x11 = isig * ((p.r - T(2)) * p.r + a * a) * ir * ir;
@@ -234,11 +254,11 @@ PHX_HD void cov_derivs(const KerrPt<T>& p, T a, Cov<T>* D1, Cov<T>* D2) {
 // Right-hand side of the geodesic equation and of the parallel transport of a polarization vector F:
 //   dk^mu/dl = -Gamma^mu_ab k^a k^b,   dF^mu/dl = -Gamma^mu_ab k^a F^b.
 // kF = false: k only (F and dF are not touched; the polarization then comes from the Walker-Penrose constant).
-template <class T, bool kF = true>
+template <class T, bool kF = true, bool kNR = false>
 PHX_HD void geodesic_accel_at(T a, const KerrPt<T>& p, const T k[4], const T F[4], T dk[4], T dF[4]) {
   Cov<T> D1, D2;
   cov_derivs(p, a, &D1, &D2);
-  const Contra<T> u = contra_metric(p, a);
+  const Contra<T> u = contra_metric<T, kNR>(p, a);
   T Pk[4], Qk[4];
   symv(D1, k, Pk);  // D1 k
   symv(D2, k, Qk);  // D2 k

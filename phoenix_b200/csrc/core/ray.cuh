@@ -190,7 +190,7 @@ struct Ray {
     if constexpr (!kLate) {
       if (L >= 0 && L != leaf) {
 #pragma unroll
-        for (int d = 0; d < 3; d++) idxc[d] = fastm::rcp(ldg(s.dxc + 3 * L + d));  // feeds only the step cap
+        for (int d = 0; d < 3; d++) idxc[d] = geo_rcp<G, kShift>(ldg(s.dxc + 3 * L + d));  // feeds only the step cap
       }
     }
     leaf = L;
@@ -270,7 +270,8 @@ struct Ray {
     G dl;
     if constexpr (!kLate) {
       // FP32 and mixed: the reciprocals folded (two divisions instead of twelve; the same rule up to rounding)
-      dl = step_size_fast(sc.stepsize, sc.inv_stepsize, x2, ck, cap ? idxc : (const G*)nullptr, sc.tiny, sc.big);
+      dl = step_size_fast<G, kShift>(sc.stepsize, sc.inv_stepsize, x2, ck, cap ? idxc : (const G*)nullptr, sc.tiny,
+                                     sc.big);
     } else {
       G dxcv[3];
       if (cap) {

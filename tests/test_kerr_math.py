@@ -160,9 +160,10 @@ SHIFT_SRC = r"""
 #include "geodesic.cuh"
 using namespace phx;
 
-// The mixed kernel's FP64 island steps with the stage trig shifted from the step start (kShift) against the direct
-// evaluation at every stage, for states near the horizon and at the step sizes the island takes; and, as the scale
-// of what rounding alone does, the direct step from a start point moved by one ulp in x1 and x2.
+// The mixed kernel's FP64 geodesic steps (kShift: stage trig shifted from the step start, Newton-refined reciprocals)
+// against the direct evaluation at every stage with exact divisions, for states near the horizon and at the step
+// sizes taken there; and, as the scale of what rounding alone does, the direct step from a start point moved by one
+// ulp in x1 and x2.
 int main() {
   uint64_t s = 0x2545F4914F6CDD1Dull;
   auto u01 = [&]() { s ^= s << 13; s ^= s >> 7; s ^= s << 17; return (double)(s >> 11) / 9007199254740992.0; };
@@ -202,7 +203,7 @@ int main() {
 
 
 def test_shifted_island_stages_match_direct(tmp_path):
-    """The shifted stages stay within what one ulp of the start point does to the direct step."""
+    """The mixed geodesic's shifted stages stay within what one ulp of the start point does to the direct step."""
     src, exe = tmp_path / "sh.cpp", tmp_path / "sh"
     src.write_text(SHIFT_SRC)
     core = os.path.join(ROOT, "phoenix_b200", "csrc", "core")
@@ -210,3 +211,44 @@ def test_shifted_island_stages_match_direct(tmp_path):
     n, worst, ulp = subprocess.check_output([str(exe)]).decode().split()
     assert int(n) > 15000, n
     assert float(worst) <= float(ulp) and float(worst) <= 1e-11, (worst, ulp)
+
+
+RCP_SRC = r"""
+#include <cmath>
+#include <cstdio>
+#include <cstdint>
+#include "defs.cuh"
+
+int main() {
+  uint64_t s = 0x9E3779B97F4A7C15ull;
+  auto u01 = [&]() { s ^= s << 13; s ^= s >> 7; s ^= s << 17; return (double)(s >> 11) / 9007199254740992.0; };
+  double worst = 0;
+  int n = 0;
+  for (int i = 0; i < 4000000; i++) {
+    const double x = (u01() < 0.5 ? -1 : 1) * std::exp((u01() - 0.5) * 2 * 69.0);  // |x| in [1e-30, 1e30]
+    const double r = phx::fastm::rcp_nr(x), q = 1.0 / x;
+    const double ulps = std::fabs(r - q) / (std::nextafter(std::fabs(q), 1e308) - std::fabs(q));
+    worst = std::fmax(worst, ulps);
+    n++;
+  }
+  const double edge[] = {0.0, -0.0, 1e-300, 1e300, -1e-40, 1e40, INFINITY};
+  int bad_edge = 0;
+  for (double x : edge) {
+    const double r = phx::fastm::rcp_nr(x), q = 1.0 / x;
+    if (!(r == q || (std::isnan(r) && std::isnan(q)))) bad_edge++;
+  }
+  std::printf("%d %.3f %d\n", n, worst, bad_edge);
+  return 0;
+}
+"""
+
+
+def test_newton_reciprocal_within_an_ulp(tmp_path):
+    """The mixed geodesic's FP64 reciprocal (core/defs.cuh rcp_nr: float seed, two Newton-Raphson steps) against the
+    IEEE quotient 1/x: within one ulp over |x| in [1e-30, 1e30], and exactly the quotient outside that range."""
+    src, exe = tmp_path / "rcp.cpp", tmp_path / "rcp"
+    src.write_text(RCP_SRC)
+    core = os.path.join(ROOT, "phoenix_b200", "csrc", "core")
+    subprocess.check_call(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-I" + core, str(src), "-o", str(exe)])
+    n, worst, bad_edge = subprocess.check_output([str(exe)]).decode().split()
+    assert int(n) == 4000000 and float(worst) <= 1.0 and int(bad_edge) == 0, (n, worst, bad_edge)
