@@ -143,7 +143,12 @@ struct Ray {
   // FP32 one-slot and all 32-slot kernels in registers.  Measured on B200: mixed 3-frequency renders 14% faster,
   // FP64 3-5%, FP32 3-frequency 3-6% (no spills at 128 registers); FP32 with one slot 3% slower, so it keeps
   // registers.
+  // Host builds (g++: tools and the host tests of this code) have no shared memory and keep the records in the object.
+#if defined(__CUDACC__)
   static constexpr bool kAccShared = (kMixed || M == Mode::kFP64 || NF > 1) && NF <= 4;
+#else
+  static constexpr bool kAccShared = false;
+#endif
   using AccStore = std::conditional_t<kAccShared, AccShared<R, kMixed, NF>, AccRegs<R, kMixed, NF>>;
   static constexpr size_t kSmemPerThread = AccStore::kSmemPerThread;
   AccStore acc;

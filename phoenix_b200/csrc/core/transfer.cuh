@@ -121,7 +121,7 @@ struct AccShared {
 #if defined(__CUDA_ARCH__)
     return reinterpret_cast<R*>(phx_dyn_smem)[(f * AccWords<kKahan>::kN + e) * blockDim.x + threadIdx.x];
 #else
-    static R unused;  // device-only storage
+    static R unused;  // the host pass of nvcc compiles this but never runs it (g++ builds keep records in registers)
     return unused;
 #endif
   }
