@@ -233,6 +233,8 @@ typedef struct {
   int32_t keep_order;      /* nonzero: tiles in item order; 0: the largest images' tiles first */
   int32_t tile_shape;      /* pixel order of the items without a job list, i.e. the shape of the pixel tile a warp's
                               32 consecutive rays cover: PHX_TILE_* (0 = Morton, the reference's schedule) */
+  int32_t lane_setup;      /* nonzero: each lane sets up the camera ray it takes (no start-state buffer); 0: a ray-setup
+                              kernel sets up every job at full SIMD width before the queue kernel, in the same graph */
 } PhxBatchOptions;
 
 /* Tile shapes: Morton (Z-order, 8x4-pixel warp tiles, the reference's host::jobs::schedule), or tiles of w x h pixels

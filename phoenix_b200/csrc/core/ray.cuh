@@ -166,9 +166,14 @@ struct Ray {
 
   PHX_HD void init(const SnapView<R, PT>& s, const SnapView<double, PT>& sd, const RenderConsts<R>& rc,
                    int32_t pixel) {
-    pix = pixel;
     const SnapView<G, PT>& sg = geo_view(s, sd);
-    const RayStart st = ray_start<G>(rc, sg.a, sg.hs, pixel);
+    init_from(ray_start<G>(rc, sg.a, sg.hs, pixel), pixel);
+  }
+
+  // Starts the ray from its camera set-up (ray_start), computed here or beforehand by the ray-setup kernel: the same
+  // out-of-line function either way, so the ray is bit-identical.
+  PHX_HD void init_from(const RayStart& st, int32_t pixel) {
+    pix = pixel;
     geo_init<G, kComp>(geo, st.ph, st.F1);
     kappa[0] = R(st.kappa[0]);
     kappa[1] = R(st.kappa[1]);

@@ -3,8 +3,10 @@
 // Creation uploads every item's constants (camera, integration, plasma, frequencies), its snapshot view and its job
 // list, allocates the results, cuts the job lists into tiles of `tile_rays` rays (the largest images first unless the
 // caller keeps its order: their long rays start early and short images fill the end), optionally autotunes the launch
-// (register-cap variant x refill period, each timed on an every-n-th-tile sample of the batch) and captures
-// [queue reset, queue kernel] into a graph that phx_batch_launch replays.
+// (register-cap variant x refill period, each timed on an every-n-th-tile sample of the batch, then the tile shapes)
+// and captures [queue reset, ray set-up of every item, queue kernel] into a graph that phx_batch_launch replays.  The
+// ray set-up (k_ray_setup, the camera photon and polarization of every job at full SIMD width) replaces the set-up a
+// lane would otherwise run alone, with most of its warp idle, each time it takes a new ray.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -38,6 +40,7 @@ struct PhxBatch {
   int32_t* jobs = nullptr;
   PhxFreqOut* out = nullptr;
   PhxSpectrum* spec = nullptr;  // per-frequency totals of one item (phx_batch_spectrum)
+  phx::RayStart* starts = nullptr;  // camera set-up of every job (job order), or null: lanes set up their rays
   size_t nrecords = 0;
   unsigned long long* item_ctr = nullptr;
   unsigned long long* ctl = nullptr;
@@ -52,6 +55,8 @@ struct PhxBatch {
   std::function<cudaError_t(const phx::TileDesc*, unsigned, phx::QueueShape, long long, cudaStream_t,
                             phx::LaunchShape*)>
       launch;
+  // launches the ray-setup kernel of every item on a stream (empty without a start-state buffer)
+  std::function<cudaError_t(cudaStream_t)> setup;
   cudaStream_t stream = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -131,6 +136,7 @@ void build_items(PhxBatch* b, const PhxBatchItem* items, int32_t nitems, const s
     h[i].snap = view_for<M, PT>(s);
     h[i].snap_d = h[i].snap.fp64_view();
     h[i].jobs = b->jobs + job_off[i];
+    h[i].starts = b->starts ? b->starts + job_off[i] : nullptr;
     h[i].out = reinterpret_cast<double*>(b->out + b->out_off[i]);
     h[i].pixstats = nullptr;
     h[i].ctr = b->item_ctr + (size_t)phx::kItemCounters * i;
@@ -144,6 +150,17 @@ void build_items(PhxBatch* b, const PhxBatchItem* items, int32_t nitems, const s
   unsigned long long* ctl = b->ctl;
   unsigned long long* counters = b->counters;
   const int tile_rays = b->tile_rays;
+  if (b->starts) {
+    std::vector<int64_t> njobs = b->njobs;
+    b->setup = [h, njobs, sms](cudaStream_t st) -> cudaError_t {
+      for (size_t i = 0; i < h.size(); i++) {
+        const cudaError_t e = phx::launch_ray_setup<M, PT>(h[i], njobs[i], sms, const_cast<phx::RayStart*>(h[i].starts),
+                                                            st);
+        if (e != cudaSuccess) return e;
+      }
+      return cudaSuccess;
+    };
+  }
   b->launch = [d, nf, sms, ctl, counters, tile_rays](const phx::TileDesc* tiles, unsigned mask, phx::QueueShape q,
                                                       long long max_rays, cudaStream_t st, phx::LaunchShape* ls) {
     phx::QueueArgs<R, PT> A;
@@ -173,6 +190,13 @@ float timed_launch(PhxBatch* b, const phx::TileDesc* tiles, int64_t ntiles, unsi
   float ms = 0.f;
   ck(cudaEventElapsedTime(&ms, b->e0, b->e1), "event time");
   return ms;
+}
+
+// Sets up every job's camera ray now (autotuning trials time the queue kernel alone).
+void run_setup(PhxBatch* b) {
+  if (!b->setup) return;
+  ck(b->setup(b->stream), "ray setup");
+  ck(cudaStreamSynchronize(b->stream), "ray setup");
 }
 
 void autotune(PhxBatch* b) {
@@ -217,6 +241,7 @@ void autotune(PhxBatch* b) {
     for (int shape = 0; shape < PHX_TILE_SHAPES; shape++) {
       if (shape == shape0) continue;
       upload_order(b, shape);
+      run_setup(b);
       const float ms = timed_launch(b, b->trial, b->ntrial, b->trial_mask, b->trial_rays, b->shape, &ls);
       record(b->shape, shape, ms);
       if (ms < best) {
@@ -234,6 +259,7 @@ void capture(PhxBatch* b) {
   ck(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed), "begin capture");
   cudaError_t e = phx::launch_queue_reset(b->ctl, b->counters, b->item_ctr, nwords, (unsigned long long)b->ntiles,
                                           b->stream);
+  if (e == cudaSuccess && b->setup) e = b->setup(b->stream);
   if (e == cudaSuccess) e = b->launch(b->tiles, b->tile_mask, b->shape, b->nrays, b->stream, &b->lshape);
   cudaGraph_t g = nullptr;
   const cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
@@ -329,6 +355,7 @@ PhxBatch* create_batch(const PhxBatchItem* items, int32_t nitems, const PhxBatch
   if (!all_jobs.empty())
     ck(cudaMemcpy(b->jobs, all_jobs.data(), all_jobs.size() * sizeof(int32_t), cudaMemcpyHostToDevice), "H2D jobs");
   b->out = b->alloc<PhxFreqOut>(nrec);
+  if (!o.lane_setup) b->starts = b->alloc<phx::RayStart>(all_jobs.size());
   ck(cudaMemset(b->out, 0, std::max<size_t>(nrec, 1) * sizeof(PhxFreqOut)), "memset results");
   b->item_ctr = b->alloc<unsigned long long>((size_t)phx::kItemCounters * nitems);
   b->ctl = b->alloc<unsigned long long>(phx::kQWords);
@@ -359,6 +386,7 @@ PhxBatch* create_batch(const PhxBatchItem* items, int32_t nitems, const PhxBatch
   b->shape = {o.blocks_per_sm > 0 ? o.blocks_per_sm
                                   : (b->precision == PHX_PREC_FP32 ? 4 : b->precision == PHX_PREC_MIXED ? 3 : 1),
              o.period > 0 ? o.period : phx::kDefaultPeriod};
+  run_setup(b.get());
   if (o.autotune && b->ntrial > 0) autotune(b.get());
   capture(b.get());
   b->tuning.blocks_per_sm = b->shape.blocks_per_sm;

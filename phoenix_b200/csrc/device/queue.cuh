@@ -52,6 +52,7 @@ struct alignas(128) ItemDesc {
   SnapView<R, PT> snap;
   SnapView<double, PT> snap_d;   // FP64 leaf geometry and constants (the mixed mode's geodesic)
   const int32_t* jobs;
+  const RayStart* starts;        // camera set-up of each job (k_ray_setup), or null: set up by the lane that takes it
   double* out;                   // FreqOut records of the image
   int32_t* pixstats;             // optional per-pixel (steps, segments, bad)
   unsigned long long* ctr;       // kItemCounters words
@@ -121,7 +122,11 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
         d = A.items + raw.x;
         const int32_t pix = d->jobs[raw.y + off];
         if (pix >= 0 && pix < d->rc.W * d->rc.H) {
-          ray.init(d->snap, d->snap_d, d->rc, pix);
+          if (d->starts) {
+            ray.init_from(d->starts[raw.y + off], pix);
+          } else {
+            ray.init(d->snap, d->snap_d, d->rc, pix);
+          }
           live = true;
         }
       }
@@ -189,6 +194,25 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
     if (f64o) atomicAdd(&A.counters[kCtrFp64Ops], f64o);
   }
 }
+
+// The camera set-up of every job of one image (the batched tile generator's ray set-up): one thread per job, all lanes
+// busy, written in job order for the queue kernel's refills to read.  G: the geodesic precision of the mode, whose
+// ray_start the march would call (the same out-of-line function, so rays start bit-identically).
+template <class G, class R>
+__global__ void __launch_bounds__(128) k_ray_setup(const __grid_constant__ RenderConsts<R> rc, G a, G hs,
+                                                   const int32_t* __restrict__ jobs, long long njobs,
+                                                   RayStart* __restrict__ out) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < njobs; k += stride) {
+    const int32_t pix = jobs[k];
+    if (pix >= 0 && pix < rc.W * rc.H) out[k] = ray_start<G>(rc, a, hs, pix);
+  }
+}
+
+// Launches k_ray_setup for one image of mode M (instantiated beside that mode's queue kernels, with their flags).
+template <Mode M, class PT>
+cudaError_t launch_ray_setup(const ItemDesc<typename Policy<M>::R, PT>& item, long long njobs, int sms,
+                             RayStart* out, cudaStream_t stream);
 
 // Launch configuration of the queue kernel (the autotuner's search space).
 struct QueueShape {

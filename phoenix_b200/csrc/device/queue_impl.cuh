@@ -64,4 +64,17 @@ cudaError_t launch_queue_nf(const QueueArgs<typename Policy<M>::R, PT>& args, in
   }
 }
 
+template <Mode M, class PT>
+cudaError_t launch_ray_setup(const ItemDesc<typename Policy<M>::R, PT>& item, long long njobs, int sms,
+                             RayStart* out, cudaStream_t stream) {
+  using R = typename Policy<M>::R;
+  using G = typename Policy<M>::G;
+  if (njobs <= 0) return cudaSuccess;
+  const long long blocks = std::min<long long>((njobs + 127) / 128, (long long)sms * 16);
+  const G a = sizeof(G) == sizeof(R) ? G(item.snap.a) : G(item.snap_d.a);
+  const G hs = sizeof(G) == sizeof(R) ? G(item.snap.hs) : G(item.snap_d.hs);
+  k_ray_setup<G, R><<<(unsigned)blocks, 128, 0, stream>>>(item.rc, a, hs, item.jobs, njobs, out);
+  return cudaGetLastError();
+}
+
 }  // namespace phx

@@ -96,7 +96,7 @@ class PhxBatchItem(C.Structure):
 class PhxBatchOptions(C.Structure):
     _fields_ = [("tile_rays", C.c_int32), ("blocks_per_sm", C.c_int32), ("period", C.c_int32),
                 ("autotune", C.c_int32), ("sample_stride", C.c_int32), ("keep_order", C.c_int32),
-                ("tile_shape", C.c_int32)]
+                ("tile_shape", C.c_int32), ("lane_setup", C.c_int32)]
 
 
 class PhxBatchTuning(C.Structure):

@@ -91,9 +91,12 @@ def test_autotuner_and_stream_launch(gpu_snapshots):
     items = [_item(gpu_snapshots, "cfg1", "fp32", inclination=float(i)) for i in (10, 50, 120, 170)]
     with P.Batch(items, autotune=True, sample_stride=4) as b:
         t = b.tuning()
-        assert t["ncand"] == 9 and len(t["candidates"]) == 9
+        # 3 register caps x 3 refill periods, then the 3 other tile shapes at the best of those
+        assert t["ncand"] == 12 and len(t["candidates"]) == 12
+        assert sorted(c["tile_shape"] for c in t["candidates"][9:]) == [1, 2, 3]
         best = min(t["candidates"], key=lambda c: c["ms"])
-        assert (t["blocks_per_sm"], t["period"]) == (best["blocks_per_sm"], best["period"])
+        assert (t["blocks_per_sm"], t["period"], t["tile_shape"]) == (best["blocks_per_sm"], best["period"],
+                                                                      best["tile_shape"])
         assert t["nrays"] == 4 * 64 * 64 and t["ntiles"] == 4 * 64 * 64 // 32
         s = torch.cuda.Stream()
         b.launch(s.cuda_stream)
@@ -102,6 +105,21 @@ def test_autotuner_and_stream_launch(gpu_snapshots):
         ref, _ = gpu_snapshots["cfg1"].render(items[0][1])
         err = flux_errors(res0, ref, items[0][1])
         assert err.max() <= 1e-4
+
+
+@pytest.mark.parametrize("precision", ["fp32", "mixed", "fp64"])
+def test_ray_setup_kernel_matches_lane_setup(gpu_snapshots, precision):
+    """The batch's ray-setup kernel (every job's camera ray at full SIMD width, before the queue kernel) starts the rays
+    exactly as a lane that sets up its own ray does: bit-identical images, for every tile shape."""
+    items = [_item(gpu_snapshots, n, precision) for n in ("thick", "edge", "cfg1")]
+    for shape in (0, 2):
+        out = []
+        for lane in (False, True):
+            with P.Batch(items, blocks_per_sm=0, period=32, tile_shape=shape, lane_setup=lane) as b:
+                b.run()
+                out.append([b.result(k)[0] for k in range(len(items))])
+        for a, c in zip(*out):
+            assert np.array_equal(a, c), (precision, shape)
 
 
 def test_batch_rejects_bad_input(gpu_snapshots):
