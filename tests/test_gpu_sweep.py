@@ -1,0 +1,76 @@
+"""The hardest images of the 128-image batching sweep (needs a GPU): high frequency and low m_unit, where the emission is
+exponentially sensitive to the electron temperature and a sample that trajectory error carries across a block face
+changes a pixel by up to 20x.
+
+Each image is rendered at full size in FP32, mixed and FP64.  The FP64 render is pinned to the FP64 oracle on a pixel
+subset (a stride, the brightest pixels, and the pixels where FP32 or mixed differ from it most); the mixed render must
+then meet the path's bars against it over the whole image: total flux I within 1e-4, Q/U/V within 1e-3 of I.  FP32 is
+rendered beside it; its error is the trajectory-error flips the mixed mode's FP64 geodesic removes, and only has to be
+finite here.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import phoenix_b200 as P
+from tests.golden.cases import DEFAULTS
+
+pytestmark = pytest.mark.gpu
+
+# sweep images (bench.py BATCH, seed 7): index -> (side, inclination, frequency, m_unit)
+SWEEP = {
+    6: (512, 119.24, 6.07e11, 1.53e17),
+    24: (256, 74.9, 5.19e11, 1.30e17),
+    104: (64, 57.1, 6.08e11, 1.07e17),
+}
+
+
+def _sweep_image(k):
+    import bench
+    im = bench.batch_images()[k]
+    side, incl, nu, mu = SWEEP[k]
+    assert im["img"] == side and abs(im["inclination"] - incl) < 0.01
+    assert abs(im["frequencies"][0] / nu - 1) < 0.01 and abs(im["m_unit"] / mu - 1) < 0.01
+    return im
+
+
+def _flux_err(res, ref, p):
+    f, g = P.flux(res, p), P.flux(ref, p)
+    return np.abs(f - g) / np.abs(g[:, :1])
+
+
+@pytest.mark.parametrize("k", sorted(SWEEP))
+def test_sweep_image_mixed_meets_the_bar(gpu_snapshots, snapshots, k):
+    from oracle.oracle import Oracle
+    im = _sweep_image(k)
+    snap = gpu_snapshots["cfg1"]
+    res = {}
+    for prec in ("fp64", "fp32", "mixed"):
+        p = P.make_params(precision=prec, **im)
+        res[prec], _ = snap.render(p)
+    p = P.make_params(precision="fp64", **im)
+    W, H = p.img_width, p.img_height
+    I64 = res["fp64"][..., 0, 0].reshape(-1)
+    # the FP64 render against the oracle on the pixels that matter for this comparison
+    worst = set()
+    for prec in ("fp32", "mixed"):
+        d = np.abs(res[prec][..., 0, 0].reshape(-1) - I64)
+        worst.update(np.argsort(d)[::-1][:16].tolist())
+    pix = np.unique(np.concatenate([np.arange(0, W * H, max(1, W * H // 400)), np.argsort(I64)[::-1][:16],
+                                    np.array(sorted(worst), dtype=np.int64)])).astype(np.int32)
+    dump, grid, spec = snapshots["cfg1"]
+    kw = dict(DEFAULTS)
+    kw.update(img_width=W, img_height=H, inclination=im["inclination"], frequencies=tuple(im["frequencies"]),
+              m_unit=im["m_unit"])
+    kw = {("phi_cam" if key == "phi" else key): v for key, v in kw.items()}
+    o = Oracle(dump, grid, nlevels=spec["nlevels"], sfc=1, **kw)
+    ref, _, _ = o.render(pix)
+    o.close()
+    got = res["fp64"].reshape(-1, 1, 6)[pix]
+    scale = np.abs(ref[:, 0, :4]).max()
+    assert np.abs(got[:, 0, :4] - ref[:, 0, :4]).max() <= 1e-9 * scale
+    # the mixed image against the (oracle-pinned) FP64 image
+    err = _flux_err(res["mixed"], res["fp64"], p)
+    assert err[:, 0].max() <= 1e-4 and err[:, 1:].max() <= 1e-3, (k, err)
+    assert np.isfinite(_flux_err(res["fp32"], res["fp64"], p)).all()
