@@ -370,7 +370,17 @@ struct Ray {
       if constexpr (sizeof(G) == sizeof(R)) {
         wp_components(s.a, pg, k, perp, para, kappa, &C, &S);
       } else {
-        const KerrPt<R> p0 = kerr_point_r(s.a, s.hs, rx, R(x0[2]));
+        // the FP64 geometry of this point, rounded (no second metric point: wp_components reads r, sin, cos, theta')
+        KerrPt<R> p0;
+        p0.r = R(pg.r);
+        p0.s = R(pg.s);
+        p0.c = R(pg.c);
+        p0.s2 = R(pg.s2);
+        p0.tp = R(pg.tp);
+        p0.tpp = R(pg.tpp);
+        p0.sig = R(pg.sig);
+        p0.isig = R(pg.isig);
+        p0.q = R(pg.q);
         wp_components(s.a, p0, k, perp, para, kappa, &C, &S);
       }
     } else {
