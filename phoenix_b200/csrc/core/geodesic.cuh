@@ -59,22 +59,28 @@ PHX_HD R pole_x2(const GeoState<R, NS>& g) {
   return g.hi[2] + (kComp ? g.lo[2] : R(0));
 }
 
-// exp(d) for |d| <= 0.1 by its Taylor series to d^11 (truncation below 3e-21 relative).
-template <class T>
+// exp(d) by its Taylor series to d^N in Horner form: N = 11 for |d| <= 0.1 (truncation below 3e-21 relative), N = 7
+// for |d| <= 0.025 (below 4e-18).
+template <class T, int N = 11>
 PHX_HD T exp_small(T d) {
   T e = T(1);
 #pragma unroll
-  for (int n = 11; n >= 1; n--) e = T(1) + d * T(1.0 / n) * e;
+  for (int n = N; n >= 1; n--) e = T(1) + d * T(1.0 / n) * e;
   return e;
 }
+
+// Largest stage offset in x1 and x2 that the shifted stages take by the short series (exp_small<7>, sincos_tiny).
+// A step changes x1 and x2 by at most about `stepsize` = 0.01 (the step-size rule), so the bound leaves 2.5x margin;
+// a larger offset evaluates the point directly.
+constexpr double kShiftMax = 0.025;
 
 // One classical RK4 step of length dt.  Stage sums are kept as (d0 + d3) and (d1 + d2) so that the update
 // ((d0 + d3) + 2 (d1 + d2)) dt/6 needs two 12-vectors instead of four.  The stage loop is deliberately not unrolled:
 // one copy of the stage body (metric, derivatives, both Christoffel contractions) keeps the march loop small enough
 // for the instruction cache, which four unrolled copies overflow.
 // kShift (uncompensated state only; the mixed mode's FP64 geodesic): each stage's exp(x1) and sincos(x2) come from the
-// step's starting point and short series of the stage offset (exp_small, sincos_small: exact to rounding for the
-// offsets allowed), one exp and one sincos per step instead of four, and the geometry's reciprocals are the
+// step's starting point and short series of the stage offset (exp_small<7>, sincos_tiny: exact to rounding for
+// offsets up to kShiftMax), one exp and one sincos per step instead of four, and the geometry's reciprocals are the
 // Newton-refined FP64 ones (fastm::rcp_nr); a stage whose offset is larger evaluates the point directly.
 template <class R, bool kComp, int NS, bool kShift = false>
 PHX_HD void rk4_step(R a, R hs, GeoState<R, NS>& g, R dt) {
@@ -107,11 +113,11 @@ PHX_HD void rk4_step(R a, R hs, GeoState<R, NS>& g, R dt) {
     d[3] = y[7];
     if constexpr (kShift) {
       const R d1 = inc[1], d2 = inc[2];
-      if (fabs_t(d1) <= R(0.1) && fabs_t(d2) <= R(0.5)) {
+      if (fabs_t(d1) <= R(kShiftMax) && fabs_t(d2) <= R(kShiftMax)) {
         R sd, cd;
-        sincos_small(d2, &sd, &cd);
+        sincos_tiny(d2, &sd, &cd);
         const KerrPt<R> p =
-            kerr_point_rsc<R, true>(a, hs, e0 * exp_small(d1), y[2], sx0 * cd + cx0 * sd, cx0 * cd - sx0 * sd);
+            kerr_point_rsc<R, true>(a, hs, e0 * exp_small<R, 7>(d1), y[2], sx0 * cd + cx0 * sd, cx0 * cd - sx0 * sd);
         geodesic_accel_at<R, kF, true>(a, p, y + 4, y + 8, d + 4, d + 8);
       } else {
         geodesic_accel<R, kF>(a, hs, y[1], y[2], y + 4, y + 8, d + 4, d + 8);

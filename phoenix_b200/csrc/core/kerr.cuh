@@ -96,6 +96,20 @@ PHX_HD T geo_div(T a, T b) {
   }
 }
 
+// sin d and cos d for |d| <= 0.025 in FP64: four Taylor terms each (truncation below 4e-19 and 4e-18).
+template <class T>
+PHX_HD void sincos_tiny(T d, T* sn, T* cs) {
+  const T z = d * d;
+  T s = T(1) - z * T(1.0 / 42.0);
+  s = T(1) - z * T(1.0 / 20.0) * s;
+  s = T(1) - z * T(1.0 / 6.0) * s;
+  T c = T(1) - z * T(1.0 / 30.0);
+  c = T(1) - z * T(1.0 / 12.0) * c;
+  c = T(1) - z * T(1.0 / 2.0) * c;
+  *sn = d * s;
+  *cs = c;
+}
+
 // Geometry at (r, x2) when r = exp(x1) and sin x2, cos x2 are already known.
 template <class T, bool kNR = false>
 PHX_HD KerrPt<T> kerr_point_rsc(T a, T hs, T r, T x2, T sx, T cx) {

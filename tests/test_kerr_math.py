@@ -184,7 +184,7 @@ int main() {
     g3 = g1;
     g3.hi[1] = std::nextafter(g3.hi[1], 1e9);
     g3.hi[2] = std::nextafter(g3.hi[2], 1e9);
-    const double dt = -(0.002 + 0.05 * u01()) * r;
+    const double dt = -(0.0005 + 0.01 * u01()) * r;  // stage offsets within the short series (|dx| < 0.025)
     rk4_step<double, false, 8, false>(a, hs, g1, dt);
     rk4_step<double, false, 8, true>(a, hs, g2, dt);
     rk4_step<double, false, 8, false>(a, hs, g3, dt);
