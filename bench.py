@@ -471,6 +471,32 @@ def run_serve(args):
                        "request_seed": SERVE["seed"], "resolutions": list(SERVE["resolutions"]),
                        "precision": "fp32", "budget_bytes": SERVE["budget"]},
             "setup_s": setup_s}
+    # the same requests rendered one after another by the plain single-image path (device buffers, CUDA events)
+    import torch
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(device=dev)
+    pj = {}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    outs = [torch.zeros((p.img_width * p.img_height, p.nfreqs, 6), dtype=torch.float64, device=dev) for p in params]
+    ctr = torch.zeros((len(params), P.NUM_COUNTERS), dtype=torch.int64, device=dev)
+    for p in params:
+        if p.img_width not in pj:
+            pj[p.img_width] = torch.from_numpy(P.schedule_morton(p.img_width, p.img_height)).to(dev)
+    for rep in range(2):  # the first pass warms up
+        ctr.zero_()
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for k, (r, p) in enumerate(zip(reqs, params)):
+                j = pj[p.img_width]
+                snaps[r["snapshot"]].render_async(p, j.data_ptr(), j.numel(), outs[k].data_ptr(), ctr[k].data_ptr(), 0,
+                                                  stream.cuda_stream)
+            e1.record(stream)
+        stream.synchronize()
+    plain_s = e0.elapsed_time(e1) * 1e-3
+    plain_steps = int(ctr[:, P.CTR["steps"]].sum())
+    nrays = sum(p.img_width * p.img_height for p in params)
+    line["plain_one_by_one"] = {"seconds": plain_s, "rays_per_s": nrays / plain_s, "ray_steps_per_s": plain_steps / plain_s}
+    del outs
     with P.Server(snaps, "fp32", memory_budget=SERVE["budget"]) as srv:
         # isolated latency of every request (alone on the server), after one warm-up request
         w = srv.submit(0, params[0])
