@@ -720,6 +720,7 @@ def main():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64", "mixed"])
     ap.add_argument("--img", type=int, default=WORKLOAD["img"], help="image side (profiling runs use smaller)")
     ap.add_argument("--period", type=int, default=0)
+    ap.add_argument("--blocks-per-sm", type=int, default=0, help="register-cap variant (0: the mode's default)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="plain", choices=["plain", "batch", "serve", "ingest", "mixed"],
@@ -768,8 +769,8 @@ def main():
     log(f"[rank {rank}] snapshot resident: {snap.nbytes() / 1e9:.3f} GB in {time.time() - t0:.1f} s")
 
     stream = torch.cuda.Stream(device=dev)
-    params = [P.make_params(inclination=i, precision=args.precision, period=args.period, **render_kwargs(w))
-              for i in w["inclinations"]]
+    params = [P.make_params(inclination=i, precision=args.precision, period=args.period,
+                            blocks_per_sm=args.blocks_per_sm, **render_kwargs(w)) for i in w["inclinations"]]
     npix = w["img"] * w["img"]
     jobs = torch.from_numpy(P.schedule_morton(w["img"], w["img"])).to(dev)
     res = [torch.zeros((npix, 1, 6), dtype=torch.float64, device=dev) for _ in params]

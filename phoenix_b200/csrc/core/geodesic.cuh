@@ -75,7 +75,7 @@ PHX_HD T exp_small(T d) {
 constexpr double kShiftMax = 0.025;
 
 // One classical RK4 step of length dt.  Stage sums are kept as (d0 + d3) and (d1 + d2) so that the update
-// ((d0 + d3) + 2 (d1 + d2)) dt/6 needs two 12-vectors instead of four.  The stage loop is deliberately not unrolled:
+// ((d0 + d3) + 2 (d1 + d2)) dt/6 needs two 12-vectors instead of four (kShift: one running sum).  The stage loop is deliberately not unrolled:
 // one copy of the stage body (metric, derivatives, both Christoffel contractions) keeps the march loop small enough
 // for the instruction cache, which four unrolled copies overflow.
 // kShift (uncompensated state only; the mixed mode's FP64 geodesic): each stage's exp(x1) and sincos(x2) come from the
@@ -130,12 +130,18 @@ PHX_HD void rk4_step(R a, R hs, GeoState<R, NS>& g, R dt) {
       d[6] = -d[6];
       if constexpr (kF) d[10] = -d[10];
     }
+    if constexpr (kShift) {
+      // one running sum d0 + 2 d1 + 2 d2 + d3 (one 8-vector of doubles fewer live through the stages)
 #pragma unroll
-    for (int i = 0; i < NS; i++) {
-      if (q == 0) s03[i] = d[i];
-      if (q == 1) s12[i] = d[i];
-      if (q == 2) s12[i] += d[i];
-      if (q == 3) s03[i] += d[i];
+      for (int i = 0; i < NS; i++) s03[i] = (q == 0 ? R(0) : s03[i]) + (q == 1 || q == 2 ? R(2) : R(1)) * d[i];
+    } else {
+#pragma unroll
+      for (int i = 0; i < NS; i++) {
+        if (q == 0) s03[i] = d[i];
+        if (q == 1) s12[i] = d[i];
+        if (q == 2) s12[i] += d[i];
+        if (q == 3) s03[i] += d[i];
+      }
     }
     if (q < 3) {
       const R wdt = (q == 2 ? R(1) : R(0.5)) * dt;
@@ -146,7 +152,7 @@ PHX_HD void rk4_step(R a, R hs, GeoState<R, NS>& g, R dt) {
   const R dt6 = dt / R(6);
 #pragma unroll
   for (int i = 0; i < NS; i++) {
-    const R du = (s03[i] + R(2) * s12[i]) * dt6;
+    const R du = (kShift ? s03[i] : s03[i] + R(2) * s12[i]) * dt6;
     if (kComp) {
       comp_add(g.hi[i], g.lo[i], du);
     } else {

@@ -51,7 +51,7 @@ constexpr int default_blocks_per_sm() {
 }
 
 // The variant for `blocks_per_sm` (0 = the mode's default).  FP64 and the 32-slot kernels are compiled uncapped only;
-// mixed offers 1 and 3.
+// mixed offers 1 and 3, and 4 with one frequency slot.
 template <Mode M, class PT, int NF>
 cudaError_t launch_nf(const MarchArgs<typename Policy<M>::R, PT>& args, int sms, int blocks_per_sm,
                       cudaStream_t stream, LaunchShape* shape) {
@@ -65,7 +65,7 @@ cudaError_t launch_nf(const MarchArgs<typename Policy<M>::R, PT>& args, int sms,
       return whole ? launch_mb<M, PT, NF, 384, 1>(args, sms, stream, shape)
                    : launch_mb<M, PT, NF, 128, 3>(args, sms, stream, shape);
     }
-    if constexpr (M == Mode::kFP32) {
+    if constexpr (M == Mode::kFP32 || (M == Mode::kMixed && NF == 1)) {
       if (bps == 4) {
         return whole ? launch_mb<M, PT, NF, 512, 1>(args, sms, stream, shape)
                      : launch_mb<M, PT, NF, 128, 4>(args, sms, stream, shape);
