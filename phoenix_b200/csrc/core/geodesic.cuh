@@ -63,15 +63,24 @@ PHX_HD R pole_x2(const GeoState<R, NS>& g) {
 // for |d| <= 0.025 (below 4e-18).
 template <class T, int N = 11>
 PHX_HD T exp_small(T d) {
-  T e = T(1);
+  if constexpr (N == 7) {
+    // Estrin's form: three levels of independent products instead of a seven-deep Horner chain
+    const T d2 = d * d, d4 = d2 * d2;
+    const T q0 = (T(1) + d) + d2 * (T(1.0 / 2.0) + d * T(1.0 / 6.0));
+    const T q1 = (T(1.0 / 24.0) + d * T(1.0 / 120.0)) + d2 * (T(1.0 / 720.0) + d * T(1.0 / 5040.0));
+    return q0 + d4 * q1;
+  } else {
+    T e = T(1);
 #pragma unroll
-  for (int n = N; n >= 1; n--) e = T(1) + d * T(1.0 / n) * e;
-  return e;
+    for (int n = N; n >= 1; n--) e = T(1) + d * T(1.0 / n) * e;
+    return e;
+  }
 }
 
 // Largest stage offset in x1 and x2 that the shifted stages take by the short series (exp_small<7>, sincos_tiny).
 // A step changes x1 and x2 by at most about `stepsize` = 0.01 (the step-size rule), so the bound leaves 2.5x margin;
-// a larger offset evaluates the point directly.
+// a larger offset (or |hslope| > 0.5, where the theta shift could exceed sincos_tiny's range) evaluates the point
+// directly.
 constexpr double kShiftMax = 0.025;
 
 // One classical RK4 step of length dt.  Stage sums are kept as (d0 + d3) and (d1 + d2) so that the update
@@ -88,10 +97,13 @@ PHX_HD void rk4_step(R a, R hs, GeoState<R, NS>& g, R dt) {
   static_assert(!(kShift && kComp), "the shifted stages need an uncompensated state");
   const R pi_hi = R(kPi), pi_lo = R(kPi - (double)R(kPi));
   const bool south = kComp && g.hi[2] > R(kHalfPi);
-  R e0 = R(0), sx0 = R(0), cx0 = R(0);
+  R e0 = R(0), sx0 = R(0), cx0 = R(0), s2x0 = R(0), st0 = R(0), ct0 = R(0);
   if constexpr (kShift) {
     e0 = exp_t(g.hi[1]);
     sincos_t(g.hi[2], &sx0, &cx0);
+    // theta at the start, theta0 = x2 + (h/2) sin 2x2: each stage's theta follows from a small shift of it
+    s2x0 = R(2) * sx0 * cx0;
+    sincos_t(g.hi[2] + R(0.5) * hs * s2x0, &st0, &ct0);
   }
   R inc[NS], s03[NS], s12[NS];
 #pragma unroll
@@ -113,11 +125,16 @@ PHX_HD void rk4_step(R a, R hs, GeoState<R, NS>& g, R dt) {
     d[3] = y[7];
     if constexpr (kShift) {
       const R d1 = inc[1], d2 = inc[2];
-      if (fabs_t(d1) <= R(kShiftMax) && fabs_t(d2) <= R(kShiftMax)) {
+      if (fabs_t(d1) <= R(kShiftMax) && fabs_t(d2) <= R(kShiftMax) && fabs_t(hs) <= R(0.5)) {
         R sd, cd;
         sincos_tiny(d2, &sd, &cd);
-        const KerrPt<R> p =
-            kerr_point_rsc<R, true>(a, hs, e0 * exp_small<R, 7>(d1), y[2], sx0 * cd + cx0 * sd, cx0 * cd - sx0 * sd);
+        const R sx = sx0 * cd + cx0 * sd, cx = cx0 * cd - sx0 * sd;
+        const R s2x = R(2) * sx * cx, c2x = (cx - sx) * (cx + sx);
+        // theta - theta0 = d2 + (h/2)(sin 2x2 - sin 2x2_0): |.| <= (1 + |h|) kShiftMax <= 0.0375
+        R sdt, cdt;
+        sincos_tiny(d2 + R(0.5) * hs * (s2x - s2x0), &sdt, &cdt);
+        const KerrPt<R> p = kerr_point_theta<R, true>(a, hs, e0 * exp_small<R, 7>(d1), s2x, c2x,
+                                                      st0 * cdt + ct0 * sdt, ct0 * cdt - st0 * sdt);
         geodesic_accel_at<R, kF, true>(a, p, y + 4, y + 8, d + 4, d + 8);
       } else {
         geodesic_accel<R, kF>(a, hs, y[1], y[2], y + 4, y + 8, d + 4, d + 8);

@@ -96,44 +96,50 @@ PHX_HD T geo_div(T a, T b) {
   }
 }
 
-// sin d and cos d for |d| <= 0.025 in FP64: four Taylor terms each (truncation below 4e-19 and 4e-18).
+// sin d and cos d for |d| <= 0.0375 in FP64: four Taylor terms each (truncation below 2e-17 and 1e-16 relative),
+// summed in Estrin's form (two levels of independent products instead of a three-deep Horner chain).
 template <class T>
 PHX_HD void sincos_tiny(T d, T* sn, T* cs) {
-  const T z = d * d;
-  T s = T(1) - z * T(1.0 / 42.0);
-  s = T(1) - z * T(1.0 / 20.0) * s;
-  s = T(1) - z * T(1.0 / 6.0) * s;
-  T c = T(1) - z * T(1.0 / 30.0);
-  c = T(1) - z * T(1.0 / 12.0) * c;
-  c = T(1) - z * T(1.0 / 2.0) * c;
+  const T z = d * d, z2 = z * z;
+  const T s = (T(1) - z * T(1.0 / 6.0)) + z2 * (T(1.0 / 120.0) - z * T(1.0 / 5040.0));
+  const T c = (T(1) - z * T(1.0 / 2.0)) + z2 * (T(1.0 / 24.0) - z * T(1.0 / 720.0));
   *sn = d * s;
   *cs = c;
 }
 
-// Geometry at (r, x2) when r = exp(x1) and sin x2, cos x2 are already known.
+// The rest of the geometry once r, sin 2x2, cos 2x2 and sin, cos of theta are known.
 template <class T, bool kNR = false>
-PHX_HD KerrPt<T> kerr_point_rsc(T a, T hs, T r, T x2, T sx, T cx) {
+PHX_HD KerrPt<T> kerr_point_theta(T a, T hs, T r, T s2x, T c2x, T st, T ct) {
   KerrPt<T> p;
   p.r = r;
-  // sin 2x2, cos 2x2 from sin x2, cos x2 (double-angle identities)
-  const T s2x = T(2) * sx * cx, c2x = (cx - sx) * (cx + sx);
-  const T d = T(0.5) * hs * s2x;  // theta = x2 + d
   p.tp = T(1) + hs * c2x;
   p.tpp = T(-2) * hs * s2x;
-  if (fabs_t(hs) <= T(1)) {
-    // sin, cos of theta by angle addition: |d| <= |hs| / 2 <= 0.5 needs no second sincos
-    T sd, cd;
-    sincos_small(d, &sd, &cd);
-    p.s = sx * cd + cx * sd;
-    p.c = cx * cd - sx * sd;
-  } else {
-    sincos_t(x2 + d, &p.s, &p.c);
-  }
+  p.s = st;
+  p.c = ct;
   p.s2 = p.s * p.s;
   p.sig = p.r * p.r + a * a * p.c * p.c;
   p.isig = geo_rcp<T, kNR>(p.sig);  // FP32: hardware reciprocal (2 ulp), FP64: exact division or Newton-refined
   p.q = T(2) * p.r * p.isig;
   return p;
+}
+
+// Geometry at (r, x2) when r = exp(x1) and sin x2, cos x2 are already known.
+template <class T, bool kNR = false>
+PHX_HD KerrPt<T> kerr_point_rsc(T a, T hs, T r, T x2, T sx, T cx) {
+  // sin 2x2, cos 2x2 from sin x2, cos x2 (double-angle identities)
+  const T s2x = T(2) * sx * cx, c2x = (cx - sx) * (cx + sx);
+  const T d = T(0.5) * hs * s2x;  // theta = x2 + d
+  T st, ct;
+  if (fabs_t(hs) <= T(1)) {
+    // sin, cos of theta by angle addition: |d| <= |hs| / 2 <= 0.5 needs no second sincos
+    T sd, cd;
+    sincos_small(d, &sd, &cd);
+    st = sx * cd + cx * sd;
+    ct = cx * cd - sx * sd;
+  } else {
+    sincos_t(x2 + d, &st, &ct);
+  }
+  return kerr_point_theta<T, kNR>(a, hs, r, s2x, c2x, st, ct);
 }
 
 // Geometry at (r, x2) when r = exp(x1) is already known.
