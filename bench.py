@@ -875,12 +875,15 @@ def main():
             "roofline": {"bound": "fp32", "achieved": fp32_achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                          "frac": fp32_achieved / fp32_peak, "traffic": traffic, "kernel": "k_march",
                          "launch_ms": kavg_s * 1e3, "flops_per_launch": flops / nlaunch,
-                         "flops_per_unit": FLOPS, "fma_pipe_active": FMA_PIPE_ACTIVE,
+                         "flops_per_unit": FLOPS,
+                         "fma_pipe_active": FMA_PIPE_ACTIVE if args.precision == "fp32" else None,
                          "note": "the march is bound by FP32 instruction issue: algorithmic FP32 flops per launch "
                                  "(per ray-step, per emitting sample, per sample-frequency, counted in the reference's "
                                  "own FP32 code) over the CUDA-event launch time; peak = FP32 FMA issue rate measured on this GPU in this run "
                                  "(phx_measure_fp32_peak); traffic = DRAM bytes per launch; fma_pipe_active = the "
-                                 "FMA-pipe share of cycles from ncu on this workload"},
+                                 "FMA-pipe share of cycles from ncu on this workload (FP32 path only; the mixed and "
+                                 "FP64 paths run their geodesic in FP64, so the same FP32-flop count over their "
+                                 "time is a lower share)"},
             "roofline_hbm": {"bound": "hbm", "achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s",
                              "frac": hbm_achieved / hbm_peak, "traffic": traffic,
                              "algorithmic_bytes_per_launch": nbytes / nlaunch,

@@ -102,7 +102,8 @@ typedef struct {
   int32_t period;      /* march passes between lane refills, 0 = default (64) */
   int32_t blocks_per_sm; /* register-cap variant, as resident warps per SM / 4 (1: up to 255 registers in 128-thread
                             blocks; 3: 168 registers, 4: 128, as one 384 / 512-thread block per SM when the job list
-                            fills every SM, else as 128-thread blocks); 0 = default (FP32 4, mixed 3, FP64 1) */
+                            fills every SM, else as 128-thread blocks); 0 = default (FP32 4; mixed 4 with one frequency, else 3;
+                            FP64 1) */
 } PhxRenderParams;
 
 /* What a render reports (a superset of the reference's device::Info, src/device/kernel.cuh:23-30). */
@@ -225,7 +226,8 @@ typedef struct {
 
 typedef struct {
   int32_t tile_rays;       /* rays per queue tile, 0 = 32 */
-  int32_t blocks_per_sm;   /* register-cap variant (FP32: 1, 3, 4; mixed 1, 3), 0 = default (FP32 4, mixed 3, FP64 1) or autotuned */
+  int32_t blocks_per_sm;   /* register-cap variant (FP32: 1, 3, 4; mixed 1, 3, and 4 with one frequency slot),
+                              0 = default (FP32 4, mixed 3, FP64 1) or autotuned */
   int32_t period;          /* march passes between lane refills, 0 = default 64 or autotuned */
   int32_t autotune;        /* nonzero: time every (blocks_per_sm, period) candidate on a sample of the batch's tiles
                               at creation, then every tile shape at the fastest of them, and keep the fastest */

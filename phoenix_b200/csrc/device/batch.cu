@@ -205,6 +205,9 @@ void autotune(PhxBatch* b) {
   if (b->precision == PHX_PREC_FP32 && b->nf_slots <= 4) {
     for (int bps : {3, 4, 1})
       for (int per : periods) cand.push_back({bps, per});
+  } else if (b->precision == PHX_PREC_MIXED && b->nf_slots == 1) {
+    for (int bps : {3, 4, 1})
+      for (int per : periods) cand.push_back({bps, per});
   } else if (b->precision == PHX_PREC_MIXED) {
     for (int bps : {3, 1})
       for (int per : periods) cand.push_back({bps, per});

@@ -43,11 +43,12 @@ cudaError_t launch_mb(const MarchArgs<typename Policy<M>::R, PT>& args, int sms,
   return cudaGetLastError();
 }
 
-// Default variant per mode (measured on B200): FP32 4 (128 registers, 16 warps); mixed 3 (168 registers, 12 warps:
-// 4% faster than uncapped in 128-thread blocks on the bench images); FP64 uncapped.
-template <Mode M>
+// Default variant per mode (measured on B200, 3 x 512^2 bench images): FP32 4 (128 registers, 16 warps); mixed with one
+// frequency slot 4 (128 registers, 140 bytes of spills: 474 ms vs 484 ms at 168 registers, 12 warps), mixed with more
+// slots 3 (4% faster than uncapped in 128-thread blocks); FP64 uncapped.
+template <Mode M, int NF>
 constexpr int default_blocks_per_sm() {
-  return M == Mode::kFP32 ? 4 : M == Mode::kMixed ? 3 : 1;
+  return M == Mode::kFP32 ? 4 : M == Mode::kMixed ? (NF == 1 ? 4 : 3) : 1;
 }
 
 // The variant for `blocks_per_sm` (0 = the mode's default).  FP64 and the 32-slot kernels are compiled uncapped only;
@@ -59,7 +60,7 @@ cudaError_t launch_nf(const MarchArgs<typename Policy<M>::R, PT>& args, int sms,
     (void)blocks_per_sm;
     return launch_mb<M, PT, NF, 128, 1>(args, sms, stream, shape);
   } else {
-    const int bps = blocks_per_sm > 0 ? blocks_per_sm : default_blocks_per_sm<M>();
+    const int bps = blocks_per_sm > 0 ? blocks_per_sm : default_blocks_per_sm<M, NF>();
     const bool whole = args.njobs >= (long long)sms * 128 * bps;  // a whole-SM block for every SM
     if (bps == 3) {
       return whole ? launch_mb<M, PT, NF, 384, 1>(args, sms, stream, shape)

@@ -41,7 +41,7 @@ cudaError_t launch_queue_mb(const QueueArgs<typename Policy<M>::R, PT>& args, in
 // Register-cap variants and block shapes as for the single-image kernel (march_impl.cuh): `blocks_per_sm` 1 -> 128-thread
 // blocks at up to 255 registers; 3 / 4 -> 168 / 128 registers as one 384 / 512-thread block per SM, or as 128-thread
 // blocks when the work (max_rays; <= 0: unbounded, a serving loop) cannot give every SM a whole block.  FP32 offers
-// 1, 3, 4; mixed 1 and 3; FP64 and 32 slots are uncapped only.
+// 1, 3, 4; mixed 1 and 3, and 4 with one frequency slot; FP64 and 32 slots are uncapped only.
 template <Mode M, class PT, int NF>
 cudaError_t launch_queue_nf(const QueueArgs<typename Policy<M>::R, PT>& args, int sms, QueueShape q,
                             long long max_rays, cudaStream_t stream, LaunchShape* shape) {
@@ -54,7 +54,7 @@ cudaError_t launch_queue_nf(const QueueArgs<typename Policy<M>::R, PT>& args, in
       return whole ? launch_queue_mb<M, PT, NF, 384, 1>(args, sms, q.period, max_rays, stream, shape)
                    : launch_queue_mb<M, PT, NF, 128, 3>(args, sms, q.period, max_rays, stream, shape);
     }
-    if constexpr (M == Mode::kFP32) {
+    if constexpr (M == Mode::kFP32 || (M == Mode::kMixed && NF == 1)) {
       if (bps == 4) {
         return whole ? launch_queue_mb<M, PT, NF, 512, 1>(args, sms, q.period, max_rays, stream, shape)
                      : launch_queue_mb<M, PT, NF, 128, 4>(args, sms, q.period, max_rays, stream, shape);
