@@ -227,7 +227,7 @@ typedef struct {
 typedef struct {
   int32_t tile_rays;       /* rays per queue tile, 0 = 32 */
   int32_t blocks_per_sm;   /* register-cap variant (FP32: 1, 3, 4; mixed 1, 3, and 4 with one frequency slot),
-                              0 = default (FP32 4, mixed 3, FP64 1) or autotuned */
+                              0 = default (FP32 4; mixed 4 with one slot, else 3; FP64 1) or autotuned */
   int32_t period;          /* march passes between lane refills, 0 = default 64 or autotuned */
   int32_t autotune;        /* nonzero: time every (blocks_per_sm, period) candidate on a sample of the batch's tiles
                               at creation, then every tile shape at the fastest of them, and keep the fastest */
@@ -302,7 +302,7 @@ typedef struct {
   int32_t max_freqs;      /* frequency slots per request (1 or 4; FP32 also up to 32), default 4 */
   int32_t tile_rays;      /* rays per queue tile, default 32 */
   int32_t period;         /* march passes between lane refills, default 64 */
-  int32_t blocks_per_sm;  /* register-cap variant, 0 = default (FP32 4, mixed 3, FP64 1) */
+  int32_t blocks_per_sm;  /* register-cap variant, 0 = default (FP32 4; mixed 4 with one slot, else 3; FP64 1) */
   int32_t max_items;      /* requests per run of the kernel before the queue is recycled, default 4096 */
   int64_t max_tiles;      /* tiles per run of the kernel, a power of two, default 2^22 */
   int32_t idle_ns;        /* sleep of an idle warp between polls of the queue, default 2000 */

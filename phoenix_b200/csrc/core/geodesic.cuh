@@ -83,6 +83,28 @@ PHX_HD T exp_small(T d) {
 // directly.
 constexpr double kShiftMax = 0.025;
 
+// One stage's derivatives with the point evaluated directly (exp and sincos of the stage's own x1, x2): the shifted
+// stages' fallback for offsets beyond kShiftMax.  Out of line (arguments and results by value): the shifted form covers
+// nearly every stage, so this second copy of the metric, its exp and its sincos stays out of the march loop (measured on
+// B200: the same step time as inlined, two registers fewer at the 168-register cap).
+template <class R>
+struct StagePoint {
+  R a, hs, x1, x2, k[4], F[4];
+};
+template <class R>
+struct StageDeriv {
+  R dk[4], dF[4];
+};
+
+template <class R, bool kF>
+PHX_HD_OUTLINE StageDeriv<R> geodesic_accel_direct(StagePoint<R> p) {
+  StageDeriv<R> o;
+#pragma unroll
+  for (int i = 0; i < 4; i++) o.dF[i] = R(0);
+  geodesic_accel<R, kF>(p.a, p.hs, p.x1, p.x2, p.k, p.F, o.dk, o.dF);
+  return o;
+}
+
 // One classical RK4 step of length dt.  Stage sums are kept as (d0 + d3) and (d1 + d2) so that the update
 // ((d0 + d3) + 2 (d1 + d2)) dt/6 needs two 12-vectors instead of four (kShift: one running sum).  The stage loop is deliberately not unrolled:
 // one copy of the stage body (metric, derivatives, both Christoffel contractions) keeps the march loop small enough
@@ -137,7 +159,22 @@ PHX_HD void rk4_step(R a, R hs, GeoState<R, NS>& g, R dt) {
                                                       st0 * cdt + ct0 * sdt, ct0 * cdt - st0 * sdt);
         geodesic_accel_at<R, kF, true>(a, p, y + 4, y + 8, d + 4, d + 8);
       } else {
-        geodesic_accel<R, kF>(a, hs, y[1], y[2], y + 4, y + 8, d + 4, d + 8);
+        StagePoint<R> sp;
+        sp.a = a;
+        sp.hs = hs;
+        sp.x1 = y[1];
+        sp.x2 = y[2];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          sp.k[i] = y[4 + i];
+          sp.F[i] = kF ? y[8 + i] : R(0);
+        }
+        const StageDeriv<R> sd = geodesic_accel_direct<R, kF>(sp);
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          d[4 + i] = sd.dk[i];
+          if constexpr (kF) d[8 + i] = sd.dF[i];
+        }
       }
     } else {
       geodesic_accel<R, kF>(a, hs, y[1], y[2], y + 4, y + 8, d + 4, d + 8);
@@ -176,31 +213,6 @@ PHX_HD void rk4_step(R a, R hs, GeoState<R, NS>& g, R dt) {
       g.hi[i] += du;
     }
   }
-}
-
-// FP64 RK4 step of an FP32 compensated state: the pair is widened to double, stepped, and split back.  Out of line
-// (state passed and returned by value): the mixed-precision island is a few percent of the steps, and its FP64 stage
-// body inlined beside the FP32 one would crowd the march loop's instruction cache.
-template <int NS>
-PHX_HD_OUTLINE GeoState<float, NS> rk4_step_widened_ool(double a, double hs, GeoState<float, NS> g, double dt) {
-  GeoState<double, NS> w;
-#pragma unroll
-  for (int i = 0; i < NS; i++) {
-    w.hi[i] = (double)g.hi[i] + (double)g.lo[i];
-    w.lo[i] = 0.0;
-  }
-  rk4_step<double, false, NS, true>(a, hs, w, dt);
-#pragma unroll
-  for (int i = 0; i < NS; i++) {
-    g.hi[i] = (float)w.hi[i];
-    g.lo[i] = (float)(w.hi[i] - (double)g.hi[i]);
-  }
-  return g;
-}
-
-template <int NS>
-PHX_HD void rk4_step_widened(double a, double hs, GeoState<float, NS>& g, double dt) {
-  g = rk4_step_widened_ool<NS>(a, hs, g, dt);
 }
 
 // RAPTOR step size (negative: the ray runs backwards from the camera), capped by a quarter of the AMR cell.

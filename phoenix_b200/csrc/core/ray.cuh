@@ -409,15 +409,16 @@ struct Ray {
         fp64 = h * kmax > rc.tau_fp64;
       }
       if (fp64) {
-        double Kd[4][4], jd[4], Ed[4][4], Sd[4];
+        SegmentIn<R> in;
+        in.h = h;
         for (int a = 0; a < 4; a++) {
-          jd[a] = jv[a];
-          for (int b = 0; b < 4; b++) Kd[a][b] = K[a][b];
+          in.j[a] = jv[a];
+          for (int b = 0; b < 4; b++) in.K[a][b] = K[a][b];
         }
-        segment_operator<double>(Kd, jd, (double)h, Ed, Sd);
+        const SegmentOut<R> o = segment_operator_fp64(in);
         for (int a = 0; a < 4; a++) {
-          Sg[a] = R(Sd[a]);
-          for (int b = 0; b < 4; b++) E[a][b] = R(Ed[a][b]);
+          Sg[a] = o.S[a];
+          for (int b = 0; b < 4; b++) E[a][b] = o.E[a][b];
         }
         ctr.fp64_ops++;
       } else {

@@ -78,6 +78,34 @@ PHX_HD void segment_operator(const R K[4][4], const R j[4], R h, R E[4][4], R S[
   }
 }
 
+// The segment operator evaluated in FP64 for a step of large optical or Faraday depth (the mixed mode; a few percent of
+// its samples).  Out of line, arguments and results by value, so that the FP64 copy of the 4x4 solve stays out of the
+// march loop beside the FP32 one.
+template <class R>
+struct SegmentIn {
+  R K[4][4], j[4], h;
+};
+template <class R>
+struct SegmentOut {
+  R E[4][4], S[4];
+};
+
+template <class R>
+PHX_HD_OUTLINE SegmentOut<R> segment_operator_fp64(SegmentIn<R> in) {
+  double K[4][4], j[4], E[4][4], S[4];
+  for (int a = 0; a < 4; a++) {
+    j[a] = in.j[a];
+    for (int b = 0; b < 4; b++) K[a][b] = in.K[a][b];
+  }
+  segment_operator<double>(K, j, (double)in.h, E, S);
+  SegmentOut<R> o;
+  for (int a = 0; a < 4; a++) {
+    o.S[a] = R(S[a]);
+    for (int b = 0; b < 4; b++) o.E[a][b] = R(E[a][b]);
+  }
+  return o;
+}
+
 template <class R>
 PHX_HD bool all_finite(const R E[4][4], const R S[4]) {
   R s = R(0);

@@ -216,15 +216,16 @@ cudaError_t launch_ray_setup(const ItemDesc<typename Policy<M>::R, PT>& item, lo
 
 // Launch configuration of the queue kernel (the autotuner's search space).
 struct QueueShape {
-  int blocks_per_sm;  // register-cap variant: 1, 3 or 4 (FP32); mixed 1 or 3; FP64 1; 0 = the mode's default
+  int blocks_per_sm;  // register-cap variant: 1, 3 or 4 (FP32); mixed 1, 3 (4 with one slot); FP64 1; 0 = default
   int period;
 };
 
-// Default register-cap variant (measured on B200): FP32 128 registers (16 warps per SM), mixed 168 (12 warps), FP64
+// Default register-cap variant (measured on B200): FP32 128 registers (16 warps per SM); mixed 128 with one frequency
+// slot (330 ms vs 368 ms at 168 registers on the 128-image sweep's autotuning sample), else 168 (12 warps); FP64
 // uncapped.
-template <Mode M>
+template <Mode M, int NF>
 constexpr int default_queue_blocks_per_sm() {
-  return M == Mode::kFP32 ? 4 : M == Mode::kMixed ? 3 : 1;
+  return M == Mode::kFP32 ? 4 : M == Mode::kMixed ? (NF == 1 ? 4 : 3) : 1;
 }
 
 // Launches the queue kernel for `nf_slots` frequency slots (1, 4 or 32) on a persistent grid (resident blocks x SMs),

@@ -48,7 +48,7 @@ cudaError_t launch_queue_nf(const QueueArgs<typename Policy<M>::R, PT>& args, in
   if constexpr (M == Mode::kFP64 || NF > 4) {
     return launch_queue_mb<M, PT, NF, 128, 1>(args, sms, q.period, max_rays, stream, shape);
   } else {
-    const int bps = q.blocks_per_sm > 0 ? q.blocks_per_sm : default_queue_blocks_per_sm<M>();
+    const int bps = q.blocks_per_sm > 0 ? q.blocks_per_sm : default_queue_blocks_per_sm<M, NF>();
     const bool whole = max_rays <= 0 || max_rays >= (long long)sms * 128 * bps;
     if (bps == 3) {
       return whole ? launch_queue_mb<M, PT, NF, 384, 1>(args, sms, q.period, max_rays, stream, shape)
