@@ -185,8 +185,7 @@ int phx_render_async(PhxSnapshot* s, const PhxRenderParams* p, const int32_t* d_
  * PHX_NOALLOC_MAX_JOBS job slots (4 MiB), which every GPU that loads the library holds until the process exits.
  * d_res: device buffer of img_width * img_height * nfreqs records.  Asynchronous on `stream` (NULL = default).
  * Rejects njobs > PHX_NOALLOC_MAX_JOBS with PHX_E_INVALID.  The first call on a device resolves the array's
- * device address with that device current; make that first call before any stream capture.  The address is kept for
- * the life of the process: do not call this entry point again on a device after cudaDeviceReset (the reset unloads
+ * device address with that device current.  The address is kept for the life of the process: do not call this entry point again on a device after cudaDeviceReset (the reset unloads
  * the library's module, and the kept address would be stale).  All calls share the
  * array (it keeps the last call's contents; the counter block is cleared before each launch), so calls that overlap
  * on the GPU race. */
