@@ -362,7 +362,7 @@ def run_batch_sweep(args):
 
     # plain path, one launch per image
     params = [P.make_params(precision="fp32", **im) for im in imgs]
-    jobs = {r: torch.from_numpy(P.schedule_morton(r, r)).to(dev) for r in BATCH["resolutions"]}
+    jobs = {r: torch.from_numpy(P.schedule_tiles(r, r, args.order)).to(dev) for r in BATCH["resolutions"]}
     outs = [torch.zeros((p.img_width * p.img_height, 1, 6), dtype=torch.float64, device=dev) for p in params]
     ctr = torch.zeros((len(params), P.NUM_COUNTERS), dtype=torch.int64, device=dev)
 
@@ -379,7 +379,8 @@ def run_batch_sweep(args):
             "warmup": W, "data": "synthetic",
             "config": {"snapshot": "64x32x32 base grid, 8^3 blocks, 3 AMR levels, seed 0", "images": len(imgs),
                        "image_seed": BATCH["seed"], "resolutions": list(BATCH["resolutions"]), "rays": rays,
-                       "l2": "flushed (256 MB write) before every timed repetition"},
+                       "l2": "flushed (256 MB write) before every timed repetition",
+                       "plain_pixel_order": args.order},
             "ray_steps": steps}
     ms = min(t_plain)
     line["plain_fp32"] = {"ms": ms, "ray_steps_per_s": steps / (ms * 1e-3), "images_per_s": len(imgs) / (ms * 1e-3),
@@ -481,7 +482,7 @@ def run_serve(args):
     ctr = torch.zeros((len(params), P.NUM_COUNTERS), dtype=torch.int64, device=dev)
     for p in params:
         if p.img_width not in pj:
-            pj[p.img_width] = torch.from_numpy(P.schedule_morton(p.img_width, p.img_height)).to(dev)
+            pj[p.img_width] = torch.from_numpy(P.schedule_tiles(p.img_width, p.img_height, args.order)).to(dev)
     for rep in range(2):  # the first pass warms up
         ctr.zero_()
         with torch.cuda.stream(stream):
@@ -651,7 +652,7 @@ def run_mixed(args):
                                            "inclination": MIXED["inclination"]}, "images": []}
     for side in MIXED["images"]:
         npix = side * side
-        jobs = torch.from_numpy(P.schedule_morton(side, side)).to(dev)
+        jobs = torch.from_numpy(P.schedule_tiles(side, side, args.order)).to(dev)
         nf = len(MIXED["frequencies"])
         row = {"image": side}
         results = {}
@@ -721,6 +722,8 @@ def main():
     ap.add_argument("--img", type=int, default=WORKLOAD["img"], help="image side (profiling runs use smaller)")
     ap.add_argument("--period", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="register-cap variant (0: the mode's default)")
+    ap.add_argument("--order", default="2x16", choices=["morton", "16x2", "32x1", "4x8", "2x16"],
+                    help="pixel order of the plain path's job lists (phx_schedule_tiles)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="plain", choices=["plain", "batch", "serve", "ingest", "mixed"],
@@ -772,7 +775,7 @@ def main():
     params = [P.make_params(inclination=i, precision=args.precision, period=args.period,
                             blocks_per_sm=args.blocks_per_sm, **render_kwargs(w)) for i in w["inclinations"]]
     npix = w["img"] * w["img"]
-    jobs = torch.from_numpy(P.schedule_morton(w["img"], w["img"])).to(dev)
+    jobs = torch.from_numpy(P.schedule_tiles(w["img"], w["img"], args.order)).to(dev)
     res = [torch.zeros((npix, 1, 6), dtype=torch.float64, device=dev) for _ in params]
     ctr = torch.zeros((len(params), P.NUM_COUNTERS), dtype=torch.int64, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
@@ -824,7 +827,7 @@ def main():
     # end to end through the public API: pinned host job list in, host FreqOut image out, every step
     e2e = None
     if not args.no_e2e:
-        jobs_h = torch.from_numpy(P.schedule_morton(w["img"], w["img"])).pin_memory()
+        jobs_h = torch.from_numpy(P.schedule_tiles(w["img"], w["img"], args.order)).pin_memory()
         outs = [torch.zeros((w["img"], w["img"], 1, 6), dtype=torch.float64).pin_memory() for _ in params]
         for k, p in enumerate(params):
             snap.render(p, jobs=jobs_h.numpy(), out=outs[k].numpy())
@@ -865,7 +868,8 @@ def main():
                                    f"primitives), 3 x {w['img']}^2 images at 10/60/163 deg, 230 GHz, m_unit 1.2e18",
                        "precision": args.precision, "images_per_step": len(params), "rays_per_step": len(params) * npix,
                        "l2": "flushed (256 MB write) before every timed step; snapshot 0.5 GB > L2",
-                       "parallelism": f"{world} GPU(s), independent replicas"},
+                       "parallelism": f"{world} GPU(s), independent replicas",
+                       "pixel_order": args.order},
             "images_per_s": nimg / (ms_max * 1e-3) * world,
             "rays_per_s": nimg * npix / (ms_max * 1e-3) * world,
             "ray_steps_per_step": steps_total / args.steps,

@@ -14,9 +14,9 @@ import numpy as np
 
 from . import native
 from .native import (CTR, NUM_COUNTERS, PREC_FP32, PREC_FP64, PREC_MIXED, PhxError, PhxRenderInfo, make_params,
-                     schedule_morton, write_output)
+                     TILE_SHAPES, schedule_morton, schedule_tiles, write_output)
 
-__all__ = ["Snapshot", "Batch", "Server", "make_params", "schedule_morton", "write_output", "flux", "pixel_solid_angle", "device_spectrum", "spectrum_rows", "measure_fp32_peak", "PhxError", "PREC_FP32",
+__all__ = ["Snapshot", "Batch", "Server", "make_params", "schedule_morton", "schedule_tiles", "TILE_SHAPES", "write_output", "flux", "pixel_solid_angle", "device_spectrum", "spectrum_rows", "measure_fp32_peak", "PhxError", "PREC_FP32",
            "PREC_FP64", "PREC_MIXED", "CTR", "NUM_COUNTERS"]
 
 G_GRAV, M_SUN, C_LIGHT, KPC, JANSKY = 6.674e-8, 1.989e33, 2.99792458e10, 3.086e21, 1e23
@@ -88,7 +88,7 @@ class Snapshot:
 
     def render(self, params=None, jobs=None, out=None, **kw):
         """Render; returns (res[img_width, img_height, nfreqs, 6] float64, info dict).  `jobs`: pixel indices
-        i * img_height + j (default every pixel, Morton order); pixels outside `jobs` keep `out`'s values."""
+        i * img_height + j (default every pixel, in the library's default pixel order); pixels outside `jobs` keep `out`'s values."""
         p = params if params is not None else make_params(**kw)
         W, H, F = p.img_width, p.img_height, p.nfreqs
         res = out if out is not None else np.zeros((W, H, F, 6), dtype=np.float64)

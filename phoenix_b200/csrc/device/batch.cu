@@ -84,25 +84,10 @@ struct PhxBatch {
 
 namespace {
 
-// Pixel order of a W x H image for a tile shape (PHX_TILE_*): Morton, or w x h tiles (j fastest inside a tile) in
-// Morton order of the tile coordinates.
+// Pixel order of a W x H image for a tile shape (PHX_TILE_*, phx_schedule_tiles).
 std::vector<int32_t> pixel_order(int32_t W, int32_t H, int shape) {
   std::vector<int32_t> m((size_t)W * H);
-  if (shape == PHX_TILE_MORTON) {
-    if (phx_schedule_morton(W, H, m.data()) != PHX_OK) throw std::runtime_error(last_error());
-    return m;
-  }
-  static const int dims[PHX_TILE_SHAPES][2] = {{8, 4}, {16, 2}, {32, 1}, {4, 8}};
-  const int tw = dims[shape][0], th = dims[shape][1];
-  const int32_t nti = (W + tw - 1) / tw, ntj = (H + th - 1) / th;
-  std::vector<int32_t> tiles((size_t)nti * ntj);
-  if (phx_schedule_morton(nti, ntj, tiles.data()) != PHX_OK) throw std::runtime_error(last_error());
-  size_t n = 0;
-  for (const int32_t t : tiles) {
-    const int32_t ti = t / ntj, tj = t % ntj;
-    for (int32_t i = ti * tw; i < std::min(W, (ti + 1) * tw); i++)
-      for (int32_t j = tj * th; j < std::min(H, (tj + 1) * th); j++) m[n++] = i * H + j;
-  }
+  if (phx_schedule_tiles(W, H, shape, m.data()) != PHX_OK) throw std::runtime_error(last_error());
   return m;
 }
 

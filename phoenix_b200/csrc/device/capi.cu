@@ -332,6 +332,26 @@ int phx_schedule_morton(int32_t W, int32_t H, int32_t* jobs) {
   });
 }
 
+int phx_schedule_tiles(int32_t W, int32_t H, int32_t shape, int32_t* jobs) {
+  if (shape == PHX_TILE_MORTON) return phx_schedule_morton(W, H, jobs);
+  return guarded([&]() -> int {
+    if (!jobs || W < 1 || H < 1 || (long long)W * H > (1LL << 31) - 1) throw std::invalid_argument("bad job list");
+    if (shape < 0 || shape >= PHX_TILE_SHAPES) throw std::invalid_argument("unknown tile_shape");
+    static const int dims[PHX_TILE_SHAPES][2] = {{8, 4}, {16, 2}, {32, 1}, {4, 8}, {2, 16}};
+    const int tw = dims[shape][0], th = dims[shape][1];
+    const int32_t nti = (W + tw - 1) / tw, ntj = (H + th - 1) / th;
+    std::vector<int32_t> tiles((size_t)nti * ntj);
+    if (phx_schedule_morton(nti, ntj, tiles.data()) != PHX_OK) throw std::runtime_error(last_error());
+    size_t n = 0;
+    for (const int32_t t : tiles) {
+      const int32_t ti = t / ntj, tj = t % ntj;
+      for (int32_t i = ti * tw; i < std::min(W, (ti + 1) * tw); i++)
+        for (int32_t j = tj * th; j < std::min(H, (tj + 1) * th); j++) jobs[n++] = i * H + j;
+    }
+    return PHX_OK;
+  });
+}
+
 int phx_render_async(PhxSnapshot* s, const PhxRenderParams* p, const int32_t* d_jobs, int64_t njobs,
                      PhxFreqOut* d_res, int32_t* d_pixstats, uint64_t* d_counters, void* stream) {
   return guarded([&]() -> int {
@@ -354,7 +374,8 @@ int phx_render(PhxSnapshot* s, const PhxRenderParams* p, const int32_t* jobs, in
     std::vector<int32_t> all;
     if (!jobs) {
       all.resize(npix);
-      if (phx_schedule_morton(p->img_width, p->img_height, all.data()) != PHX_OK) throw std::runtime_error(last_error());
+      if (phx_schedule_tiles(p->img_width, p->img_height, PHX_DEFAULT_PIXEL_ORDER, all.data()) != PHX_OK)
+        throw std::runtime_error(last_error());
       jobs = all.data();
       njobs = npix;
     }

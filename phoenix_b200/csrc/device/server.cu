@@ -268,7 +268,8 @@ bool PhxServer::admit_one(Request& r) {
   if (jt == job_tables.end()) {
     if (!alloc->alloc((size_t)npix * sizeof(int32_t), &jobs_off)) return false;
     std::vector<int32_t> m((size_t)npix);
-    if (phx_schedule_morton(r.p.img_width, r.p.img_height, m.data()) != PHX_OK) throw std::runtime_error(last_error());
+    if (phx_schedule_tiles(r.p.img_width, r.p.img_height, PHX_DEFAULT_PIXEL_ORDER, m.data()) != PHX_OK)
+      throw std::runtime_error(last_error());
     ck(cudaMemcpyAsync(arena + jobs_off, m.data(), m.size() * sizeof(int32_t), cudaMemcpyHostToDevice, control),
        "H2D jobs");
     ck(cudaStreamSynchronize(control), "H2D jobs");

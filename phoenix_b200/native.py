@@ -26,7 +26,7 @@ CTR = dict(queue=0, steps=1, nplasma=2, bad=3, scans=4, fp64_steps=5, fp64_ops=6
 
 # Every symbol include/phoenix_b200.h declares.
 EXPORTS = ["phx_default_params", "phx_snapshot_create", "phx_snapshot_load", "phx_snapshot_destroy",
-           "phx_bhac_read", "phx_bhac_describe", "phx_bhac_free", "phx_snapshot_bytes", "phx_schedule_morton", "phx_render", "phx_render_async", "phx_render_noalloc", "phx_write_output", "phx_last_error",
+           "phx_bhac_read", "phx_bhac_describe", "phx_bhac_free", "phx_snapshot_bytes", "phx_schedule_morton", "phx_schedule_tiles", "phx_render", "phx_render_async", "phx_render_noalloc", "phx_write_output", "phx_last_error",
            "phx_version", "phx_default_batch_options", "phx_batch_create", "phx_batch_launch", "phx_batch_run",
            "phx_batch_result", "phx_batch_device_result", "phx_batch_tuning", "phx_batch_destroy",
            "phx_default_server_options", "phx_server_create", "phx_server_submit", "phx_server_poll",
@@ -190,6 +190,7 @@ def lib():
     L.phx_snapshot_bytes.argtypes = [C.c_void_p]
     L.phx_snapshot_bytes.restype = C.c_int64
     L.phx_schedule_morton.argtypes = [C.c_int32, C.c_int32, C.c_void_p]
+    L.phx_schedule_tiles.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_void_p]
     L.phx_render.argtypes = [C.c_void_p, P(PhxRenderParams), C.c_void_p, C.c_int64, C.c_void_p, P(PhxRenderInfo)]
     L.phx_render_async.argtypes = [C.c_void_p, P(PhxRenderParams), C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p]
@@ -229,7 +230,7 @@ def lib():
                  "phx_server_stats"):
         getattr(L, name).restype = C.c_int
     for name in ("phx_snapshot_create", "phx_snapshot_load", "phx_bhac_read", "phx_bhac_describe", "phx_schedule_morton",
-                 "phx_render", "phx_render_async", "phx_render_noalloc", "phx_batch_create", "phx_batch_launch",
+                 "phx_schedule_tiles", "phx_render", "phx_render_async", "phx_render_noalloc", "phx_batch_create", "phx_batch_launch",
                  "phx_batch_run", "phx_batch_result", "phx_batch_device_result", "phx_batch_tuning",
                  "phx_batch_spectrum", "phx_spectrum_async", "phx_measure_fp32_peak"):
         getattr(L, name).restype = C.c_int
@@ -269,6 +270,18 @@ def make_params(**kw) -> PhxRenderParams:
 def schedule_morton(width: int, height: int) -> np.ndarray:
     jobs = np.empty(width * height, dtype=np.int32)
     check(lib().phx_schedule_morton(width, height, jobs.ctypes.data))
+    return jobs
+
+
+# pixel orders (PHX_TILE_*): Morton, or w x h tiles (w along i, h along j) in Morton order of the tiles
+TILE_SHAPES = {"morton": 0, "16x2": 1, "32x1": 2, "4x8": 3, "2x16": 4}
+
+
+def schedule_tiles(width: int, height: int, shape="morton") -> np.ndarray:
+    """Pixel job list in the order of a tile shape (a TILE_SHAPES name or PHX_TILE_* number)."""
+    code = TILE_SHAPES[shape] if isinstance(shape, str) else int(shape)
+    jobs = np.empty(width * height, dtype=np.int32)
+    check(lib().phx_schedule_tiles(width, height, code, jobs.ctypes.data))
     return jobs
 
 

@@ -47,6 +47,24 @@ def test_morton_schedule(built, wh):
     assert np.array_equal(native.schedule_morton(*wh), _schedule_reference_order(*wh))
 
 
+@pytest.mark.parametrize("shape,tw,th", [("16x2", 16, 2), ("32x1", 32, 1), ("4x8", 4, 8), ("2x16", 2, 16)])
+@pytest.mark.parametrize("wh", [(1, 1), (13, 7), (64, 64), (96, 40)])
+def test_tile_schedules(built, shape, tw, th, wh):
+    """Every pixel once; the image cut into tw x th tiles (j fastest inside one), the tiles in Morton order."""
+    W, H = wh
+    jobs = native.schedule_tiles(W, H, shape)
+    assert np.array_equal(np.sort(jobs), np.arange(W * H))
+    nti, ntj = -(-W // tw), -(-H // th)
+    want = []
+    for t in _schedule_reference_order(nti, ntj):
+        ti, tj = divmod(int(t), ntj)
+        want += [i * H + j for i in range(ti * tw, min(W, (ti + 1) * tw)) for j in range(tj * th, min(H, (tj + 1) * th))]
+    assert np.array_equal(jobs, np.array(want, dtype=np.int32))
+    assert np.array_equal(native.schedule_tiles(W, H, "morton"), native.schedule_morton(W, H))
+    with pytest.raises(native.PhxError):
+        native.schedule_tiles(W, H, 9)
+
+
 def _read_host(dump, grid, spec, f64=True):
     L = native.lib()
     opt = native.PhxReadOptions(3, 1, 1 if spec["sfc"] else 0, spec["nlevels"])
