@@ -68,6 +68,20 @@ def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
+def job_list(P, p, order):
+    """The plain path's job list of an image: the library's default pixel order for it ("auto": 2x16 tiles near
+    face-on, Morton otherwise) or a named tile order."""
+    shape = P.default_pixel_order(p) if order == "auto" else order
+    return P.schedule_tiles(p.img_width, p.img_height, shape)
+
+
+def order_desc(P, params, order):
+    if order != "auto":
+        return order
+    names = {v: k for k, v in P.TILE_SHAPES.items()}
+    return "auto: " + ", ".join(names[P.default_pixel_order(p)] for p in params)
+
+
 def generated_snapshot(gen_args, root=None):
     """Generate (once per machine) a synthetic BHAC snapshot with phx_gen_snapshot; returns (dump, grid)."""
     key = hashlib.sha1(json.dumps(list(gen_args)).encode()).hexdigest()[:12]
@@ -362,14 +376,14 @@ def run_batch_sweep(args):
 
     # plain path, one launch per image
     params = [P.make_params(precision="fp32", **im) for im in imgs]
-    jobs = {r: torch.from_numpy(P.schedule_tiles(r, r, args.order)).to(dev) for r in BATCH["resolutions"]}
+    jobs = [torch.from_numpy(job_list(P, p, args.order)).to(dev) for p in params]
     outs = [torch.zeros((p.img_width * p.img_height, 1, 6), dtype=torch.float64, device=dev) for p in params]
     ctr = torch.zeros((len(params), P.NUM_COUNTERS), dtype=torch.int64, device=dev)
 
     def plain():
         ctr.zero_()
         for k, p in enumerate(params):
-            j = jobs[p.img_width]
+            j = jobs[k]
             snap.render_async(p, j.data_ptr(), j.numel(), outs[k].data_ptr(), ctr[k].data_ptr(), 0, stream.cuda_stream)
 
     t_plain = timed(plain)
@@ -481,14 +495,15 @@ def run_serve(args):
     outs = [torch.zeros((p.img_width * p.img_height, p.nfreqs, 6), dtype=torch.float64, device=dev) for p in params]
     ctr = torch.zeros((len(params), P.NUM_COUNTERS), dtype=torch.int64, device=dev)
     for p in params:
-        if p.img_width not in pj:
-            pj[p.img_width] = torch.from_numpy(P.schedule_tiles(p.img_width, p.img_height, args.order)).to(dev)
+        key = (p.img_width, P.default_pixel_order(p) if args.order == "auto" else args.order)
+        if key not in pj:
+            pj[key] = torch.from_numpy(job_list(P, p, args.order)).to(dev)
     for rep in range(2):  # the first pass warms up
         ctr.zero_()
         with torch.cuda.stream(stream):
             e0.record(stream)
             for k, (r, p) in enumerate(zip(reqs, params)):
-                j = pj[p.img_width]
+                j = pj[(p.img_width, P.default_pixel_order(p) if args.order == "auto" else args.order)]
                 snaps[r["snapshot"]].render_async(p, j.data_ptr(), j.numel(), outs[k].data_ptr(), ctr[k].data_ptr(), 0,
                                                   stream.cuda_stream)
             e1.record(stream)
@@ -652,13 +667,13 @@ def run_mixed(args):
                                            "inclination": MIXED["inclination"]}, "images": []}
     for side in MIXED["images"]:
         npix = side * side
-        jobs = torch.from_numpy(P.schedule_tiles(side, side, args.order)).to(dev)
         nf = len(MIXED["frequencies"])
         row = {"image": side}
         results = {}
         for prec in ("fp64", "fp32", "mixed"):
             p = P.make_params(precision=prec, img=side, frequencies=list(MIXED["frequencies"]),
                               m_unit=MIXED["m_unit"], inclination=MIXED["inclination"])
+            jobs = torch.from_numpy(job_list(P, p, args.order)).to(dev)
             res = torch.zeros((npix, nf, 6), dtype=torch.float64, device=dev)
             ctr = torch.zeros(P.NUM_COUNTERS, dtype=torch.int64, device=dev)
             best = None
@@ -722,8 +737,9 @@ def main():
     ap.add_argument("--img", type=int, default=WORKLOAD["img"], help="image side (profiling runs use smaller)")
     ap.add_argument("--period", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="register-cap variant (0: the mode's default)")
-    ap.add_argument("--order", default="2x16", choices=["morton", "16x2", "32x1", "4x8", "2x16"],
-                    help="pixel order of the plain path's job lists (phx_schedule_tiles)")
+    ap.add_argument("--order", default="auto", choices=["auto", "morton", "16x2", "32x1", "4x8", "2x16"],
+                    help="pixel order of the plain path's job lists: the library's per-image default "
+                         "(phx_default_pixel_order) or a named tile order (phx_schedule_tiles)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="plain", choices=["plain", "batch", "serve", "ingest", "mixed"],
@@ -775,7 +791,7 @@ def main():
     params = [P.make_params(inclination=i, precision=args.precision, period=args.period,
                             blocks_per_sm=args.blocks_per_sm, **render_kwargs(w)) for i in w["inclinations"]]
     npix = w["img"] * w["img"]
-    jobs = torch.from_numpy(P.schedule_tiles(w["img"], w["img"], args.order)).to(dev)
+    jobs = [torch.from_numpy(job_list(P, p, args.order)).to(dev) for p in params]
     res = [torch.zeros((npix, 1, 6), dtype=torch.float64, device=dev) for _ in params]
     ctr = torch.zeros((len(params), P.NUM_COUNTERS), dtype=torch.int64, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
@@ -783,7 +799,7 @@ def main():
     def one_step():
         ctr.zero_()
         for k, p in enumerate(params):
-            snap.render_async(p, jobs.data_ptr(), npix, res[k].data_ptr(), ctr[k].data_ptr(), 0, stream.cuda_stream)
+            snap.render_async(p, jobs[k].data_ptr(), npix, res[k].data_ptr(), ctr[k].data_ptr(), 0, stream.cuda_stream)
 
     # the FP32 roofline's denominator, measured on this GPU before the timed region
     fp32_peak = P.measure_fp32_peak() if rank == 0 else 0.0
@@ -808,7 +824,7 @@ def main():
                 ctr.zero_()
                 for k, p in enumerate(params):
                     kev[s][k][0].record(stream)
-                    snap.render_async(p, jobs.data_ptr(), npix, res[k].data_ptr(), ctr[k].data_ptr(), 0,
+                    snap.render_async(p, jobs[k].data_ptr(), npix, res[k].data_ptr(), ctr[k].data_ptr(), 0,
                                       stream.cuda_stream)
                     kev[s][k][1].record(stream)
                 ev[s][1].record(stream)
@@ -827,10 +843,10 @@ def main():
     # end to end through the public API: pinned host job list in, host FreqOut image out, every step
     e2e = None
     if not args.no_e2e:
-        jobs_h = torch.from_numpy(P.schedule_tiles(w["img"], w["img"], args.order)).pin_memory()
+        jobs_h = [torch.from_numpy(job_list(P, p, args.order)).pin_memory() for p in params]
         outs = [torch.zeros((w["img"], w["img"], 1, 6), dtype=torch.float64).pin_memory() for _ in params]
         for k, p in enumerate(params):
-            snap.render(p, jobs=jobs_h.numpy(), out=outs[k].numpy())
+            snap.render(p, jobs=jobs_h[k].numpy(), out=outs[k].numpy())
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
@@ -838,7 +854,7 @@ def main():
         t1 = time.perf_counter()
         for _ in range(args.steps):
             for k, p in enumerate(params):
-                _, info = snap.render(p, jobs=jobs_h.numpy(), out=outs[k].numpy())
+                _, info = snap.render(p, jobs=jobs_h[k].numpy(), out=outs[k].numpy())
                 e_steps += info["steps"]
         e_s = time.perf_counter() - t1
         te_max, ne_all = max_time_sum_work(e_s, e_steps, dev, world)
@@ -869,7 +885,7 @@ def main():
                        "precision": args.precision, "images_per_step": len(params), "rays_per_step": len(params) * npix,
                        "l2": "flushed (256 MB write) before every timed step; snapshot 0.5 GB > L2",
                        "parallelism": f"{world} GPU(s), independent replicas",
-                       "pixel_order": args.order},
+                       "pixel_order": order_desc(P, params, args.order)},
             "images_per_s": nimg / (ms_max * 1e-3) * world,
             "rays_per_s": nimg * npix / (ms_max * 1e-3) * world,
             "ray_steps_per_step": steps_total / args.steps,

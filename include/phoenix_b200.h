@@ -170,7 +170,7 @@ int phx_schedule_morton(int32_t img_width, int32_t img_height, int32_t* jobs);
  * the reference, whose schedule is Morton only. */
 int phx_schedule_tiles(int32_t img_width, int32_t img_height, int32_t tile_shape, int32_t* jobs);
 
-/* Renders the pixels `jobs` (host array, NULL = every pixel in PHX_DEFAULT_PIXEL_ORDER) into the host array res
+/* Renders the pixels `jobs` (host array, NULL = every pixel in phx_default_pixel_order's order) into the host array res
  * (img_width * img_height * nfreqs records, index (i * img_height + j) * nfreqs + f; pixels not in jobs are left
  * untouched).  Synchronous.  Replaces device::render (src/device/kernel.cu:284-360). */
 int phx_render(PhxSnapshot* s, const PhxRenderParams* p, const int32_t* jobs, int64_t njobs, PhxFreqOut* res,
@@ -254,10 +254,12 @@ enum {
   PHX_TILE_2X16 = 4,
   PHX_TILE_SHAPES = 5
 };
-/* The pixel order phx_render uses when it is given no job list, and the serving loop for every request: 2 x 16
- * tiles.  On B200 the single-image kernel ran 4% faster in FP32 and 7% in mixed precision with it than with Morton
- * order on 3 x 512^2 images; a pixel's result does not depend on the order. */
-#define PHX_DEFAULT_PIXEL_ORDER PHX_TILE_2X16
+/* The pixel order (PHX_TILE_*) for an image, which phx_render uses when it is given no job list and the serving loop
+ * uses for every request: 2 x 16 tiles when the camera is within about 41 degrees of the spin axis (|cos inclination|
+ * >= 0.75), else Morton.  A pixel's result does not depend on the order, only the warps' coherence does: on B200, FP32
+ * 512^2 images, 2 x 16 tiles ran 3-10 % faster than Morton at inclinations up to 35 and from 145 degrees, and up to 25
+ * % slower near edge-on (75-105 degrees).  Returns PHX_TILE_MORTON for a null p. */
+int phx_default_pixel_order(const PhxRenderParams* p);
 
 #define PHX_TUNE_MAX_CANDIDATES 16
 typedef struct {

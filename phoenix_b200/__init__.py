@@ -14,9 +14,9 @@ import numpy as np
 
 from . import native
 from .native import (CTR, NUM_COUNTERS, PREC_FP32, PREC_FP64, PREC_MIXED, PhxError, PhxRenderInfo, make_params,
-                     TILE_SHAPES, schedule_morton, schedule_tiles, write_output)
+                     TILE_SHAPES, default_pixel_order, schedule_morton, schedule_tiles, write_output)
 
-__all__ = ["Snapshot", "Batch", "Server", "make_params", "schedule_morton", "schedule_tiles", "TILE_SHAPES", "write_output", "flux", "pixel_solid_angle", "device_spectrum", "spectrum_rows", "measure_fp32_peak", "PhxError", "PREC_FP32",
+__all__ = ["Snapshot", "Batch", "Server", "make_params", "schedule_morton", "schedule_tiles", "default_pixel_order", "TILE_SHAPES", "write_output", "flux", "pixel_solid_angle", "device_spectrum", "spectrum_rows", "measure_fp32_peak", "PhxError", "PREC_FP32",
            "PREC_FP64", "PREC_MIXED", "CTR", "NUM_COUNTERS"]
 
 G_GRAV, M_SUN, C_LIGHT, KPC, JANSKY = 6.674e-8, 1.989e33, 2.99792458e10, 3.086e21, 1e23

@@ -332,6 +332,12 @@ int phx_schedule_morton(int32_t W, int32_t H, int32_t* jobs) {
   });
 }
 
+int phx_default_pixel_order(const PhxRenderParams* p) {
+  if (!p) return PHX_TILE_MORTON;
+  const double c = std::cos(p->inclination * (phx::kPi / 180.0));
+  return std::fabs(c) >= 0.75 ? PHX_TILE_2X16 : PHX_TILE_MORTON;
+}
+
 int phx_schedule_tiles(int32_t W, int32_t H, int32_t shape, int32_t* jobs) {
   if (shape == PHX_TILE_MORTON) return phx_schedule_morton(W, H, jobs);
   return guarded([&]() -> int {
@@ -374,7 +380,7 @@ int phx_render(PhxSnapshot* s, const PhxRenderParams* p, const int32_t* jobs, in
     std::vector<int32_t> all;
     if (!jobs) {
       all.resize(npix);
-      if (phx_schedule_tiles(p->img_width, p->img_height, PHX_DEFAULT_PIXEL_ORDER, all.data()) != PHX_OK)
+      if (phx_schedule_tiles(p->img_width, p->img_height, phx_default_pixel_order(p), all.data()) != PHX_OK)
         throw std::runtime_error(last_error());
       jobs = all.data();
       njobs = npix;

@@ -27,6 +27,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <tuple>
 #include <unordered_map>
 #include <vector>
 
@@ -122,7 +123,7 @@ struct PhxServer {
   int32_t* done_dev = nullptr;
   unsigned char* staging = nullptr;  // pinned: one descriptor + a request's tiles + the tail word
   size_t staging_bytes = 0;
-  std::map<std::pair<int32_t, int32_t>, size_t> job_tables;  // Morton job list per image size (arena offset)
+  std::map<std::tuple<int32_t, int32_t, int>, size_t> job_tables;  // job list per (size, pixel order): arena offset
   cudaStream_t compute = nullptr, control = nullptr, copy = nullptr;
   cudaEvent_t kernel_done = nullptr;
   // writes request r's item descriptor into dst (sizeof descriptor bytes)
@@ -262,13 +263,14 @@ bool PhxServer::admit_one(Request& r) {
   const int64_t npix = (int64_t)r.p.img_width * r.p.img_height;
   const int64_t ntiles = (npix + o.tile_rays - 1) / o.tile_rays;
   if (next_slot >= o.max_items || (long long)(tiles_reserved + ntiles) > o.max_tiles) return false;
-  const auto key = std::make_pair(r.p.img_width, r.p.img_height);
+  const int order = phx_default_pixel_order(&r.p);
+  const auto key = std::make_tuple(r.p.img_width, r.p.img_height, order);
   size_t jobs_off = 0;
   auto jt = job_tables.find(key);
   if (jt == job_tables.end()) {
     if (!alloc->alloc((size_t)npix * sizeof(int32_t), &jobs_off)) return false;
     std::vector<int32_t> m((size_t)npix);
-    if (phx_schedule_tiles(r.p.img_width, r.p.img_height, PHX_DEFAULT_PIXEL_ORDER, m.data()) != PHX_OK)
+    if (phx_schedule_tiles(r.p.img_width, r.p.img_height, order, m.data()) != PHX_OK)
       throw std::runtime_error(last_error());
     ck(cudaMemcpyAsync(arena + jobs_off, m.data(), m.size() * sizeof(int32_t), cudaMemcpyHostToDevice, control),
        "H2D jobs");

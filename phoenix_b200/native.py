@@ -26,7 +26,7 @@ CTR = dict(queue=0, steps=1, nplasma=2, bad=3, scans=4, fp64_steps=5, fp64_ops=6
 
 # Every symbol include/phoenix_b200.h declares.
 EXPORTS = ["phx_default_params", "phx_snapshot_create", "phx_snapshot_load", "phx_snapshot_destroy",
-           "phx_bhac_read", "phx_bhac_describe", "phx_bhac_free", "phx_snapshot_bytes", "phx_schedule_morton", "phx_schedule_tiles", "phx_render", "phx_render_async", "phx_render_noalloc", "phx_write_output", "phx_last_error",
+           "phx_bhac_read", "phx_bhac_describe", "phx_bhac_free", "phx_snapshot_bytes", "phx_schedule_morton", "phx_schedule_tiles", "phx_default_pixel_order", "phx_render", "phx_render_async", "phx_render_noalloc", "phx_write_output", "phx_last_error",
            "phx_version", "phx_default_batch_options", "phx_batch_create", "phx_batch_launch", "phx_batch_run",
            "phx_batch_result", "phx_batch_device_result", "phx_batch_tuning", "phx_batch_destroy",
            "phx_default_server_options", "phx_server_create", "phx_server_submit", "phx_server_poll",
@@ -191,6 +191,8 @@ def lib():
     L.phx_snapshot_bytes.restype = C.c_int64
     L.phx_schedule_morton.argtypes = [C.c_int32, C.c_int32, C.c_void_p]
     L.phx_schedule_tiles.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_void_p]
+    L.phx_default_pixel_order.argtypes = [C.c_void_p]
+    L.phx_default_pixel_order.restype = C.c_int
     L.phx_render.argtypes = [C.c_void_p, P(PhxRenderParams), C.c_void_p, C.c_int64, C.c_void_p, P(PhxRenderInfo)]
     L.phx_render_async.argtypes = [C.c_void_p, P(PhxRenderParams), C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p]
@@ -283,6 +285,11 @@ def schedule_tiles(width: int, height: int, shape="morton") -> np.ndarray:
     jobs = np.empty(width * height, dtype=np.int32)
     check(lib().phx_schedule_tiles(width, height, code, jobs.ctypes.data))
     return jobs
+
+
+def default_pixel_order(params) -> int:
+    """The library's pixel order (PHX_TILE_*) for an image: 2x16 tiles near face-on, else Morton."""
+    return lib().phx_default_pixel_order(C.byref(params))
 
 
 def write_output(res, params, outdir: str, image: str = "hdf5", block_size: int = 10):

@@ -65,6 +65,16 @@ def test_tile_schedules(built, shape, tw, th, wh):
         native.schedule_tiles(W, H, 9)
 
 
+def test_default_pixel_order(built):
+    """2x16 tiles within about 41 degrees of the spin axis (|cos i| >= 0.75), Morton elsewhere."""
+    got = {i: native.default_pixel_order(native.make_params(inclination=i)) for i in (0, 10, 35, 41, 42, 60, 90, 120,
+                                                                                     138, 140, 163, 180)}
+    two, mort = native.TILE_SHAPES["2x16"], native.TILE_SHAPES["morton"]
+    assert got == {0: two, 10: two, 35: two, 41: two, 42: mort, 60: mort, 90: mort, 120: mort, 138: mort, 140: two,
+                   163: two, 180: two}
+    assert native.lib().phx_default_pixel_order(None) == mort
+
+
 def _read_host(dump, grid, spec, f64=True):
     L = native.lib()
     opt = native.PhxReadOptions(3, 1, 1 if spec["sfc"] else 0, spec["nlevels"])
