@@ -69,8 +69,8 @@ def log(*a):
 
 
 def job_list(P, p, order):
-    """The plain path's job list of an image: the library's default pixel order for it ("auto": 2x16 tiles near
-    face-on, Morton otherwise) or a named tile order."""
+    """The plain path's job list of an image: the library's default pixel order for it ("auto": 4x8 tiles, centre
+    first) or a named tile order."""
     shape = P.default_pixel_order(p) if order == "auto" else order
     return P.schedule_tiles(p.img_width, p.img_height, shape)
 
@@ -737,7 +737,7 @@ def main():
     ap.add_argument("--img", type=int, default=WORKLOAD["img"], help="image side (profiling runs use smaller)")
     ap.add_argument("--period", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="register-cap variant (0: the mode's default)")
-    ap.add_argument("--order", default="auto", choices=["auto", "morton", "16x2", "32x1", "4x8", "2x16"],
+    ap.add_argument("--order", default="auto", choices=["auto", "morton", "16x2", "32x1", "4x8", "2x16", "center4x8"],
                     help="pixel order of the plain path's job lists: the library's per-image default "
                          "(phx_default_pixel_order) or a named tile order (phx_schedule_tiles)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")

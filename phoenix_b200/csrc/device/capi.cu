@@ -332,22 +332,28 @@ int phx_schedule_morton(int32_t W, int32_t H, int32_t* jobs) {
   });
 }
 
-int phx_default_pixel_order(const PhxRenderParams* p) {
-  if (!p) return PHX_TILE_MORTON;
-  const double c = std::cos(p->inclination * (phx::kPi / 180.0));
-  return std::fabs(c) >= 0.75 ? PHX_TILE_2X16 : PHX_TILE_MORTON;
-}
+int phx_default_pixel_order(const PhxRenderParams*) { return PHX_TILE_CENTER_4X8; }
 
 int phx_schedule_tiles(int32_t W, int32_t H, int32_t shape, int32_t* jobs) {
   if (shape == PHX_TILE_MORTON) return phx_schedule_morton(W, H, jobs);
   return guarded([&]() -> int {
     if (!jobs || W < 1 || H < 1 || (long long)W * H > (1LL << 31) - 1) throw std::invalid_argument("bad job list");
     if (shape < 0 || shape >= PHX_TILE_SHAPES) throw std::invalid_argument("unknown tile_shape");
-    static const int dims[PHX_TILE_SHAPES][2] = {{8, 4}, {16, 2}, {32, 1}, {4, 8}, {2, 16}};
+    static const int dims[PHX_TILE_SHAPES][2] = {{8, 4}, {16, 2}, {32, 1}, {4, 8}, {2, 16}, {4, 8}};
     const int tw = dims[shape][0], th = dims[shape][1];
     const int32_t nti = (W + tw - 1) / tw, ntj = (H + th - 1) / th;
     std::vector<int32_t> tiles((size_t)nti * ntj);
     if (phx_schedule_morton(nti, ntj, tiles.data()) != PHX_OK) throw std::runtime_error(last_error());
+    if (shape == PHX_TILE_CENTER_4X8) {
+      // tiles by the distance of their centre from the image centre (in pixels), nearest first; ties in Morton order
+      auto d2 = [&](int32_t t) {
+        const int32_t ti = t / ntj, tj = t % ntj;
+        const double ci = 0.5 * (ti * tw + std::min(W, (ti + 1) * tw)) - 0.5 * W;
+        const double cj = 0.5 * (tj * th + std::min(H, (tj + 1) * th)) - 0.5 * H;
+        return ci * ci + cj * cj;
+      };
+      std::stable_sort(tiles.begin(), tiles.end(), [&](int32_t a, int32_t b) { return d2(a) < d2(b); });
+    }
     size_t n = 0;
     for (const int32_t t : tiles) {
       const int32_t ti = t / ntj, tj = t % ntj;

@@ -275,8 +275,9 @@ def schedule_morton(width: int, height: int) -> np.ndarray:
     return jobs
 
 
-# pixel orders (PHX_TILE_*): Morton, or w x h tiles (w along i, h along j) in Morton order of the tiles
-TILE_SHAPES = {"morton": 0, "16x2": 1, "32x1": 2, "4x8": 3, "2x16": 4}
+# pixel orders (PHX_TILE_*): Morton, or w x h tiles (w along i, h along j) in Morton order of the tiles, or 4x8 tiles
+# by the distance of their centre from the image centre
+TILE_SHAPES = {"morton": 0, "16x2": 1, "32x1": 2, "4x8": 3, "2x16": 4, "center4x8": 5}
 
 
 def schedule_tiles(width: int, height: int, shape="morton") -> np.ndarray:
@@ -288,7 +289,7 @@ def schedule_tiles(width: int, height: int, shape="morton") -> np.ndarray:
 
 
 def default_pixel_order(params) -> int:
-    """The library's pixel order (PHX_TILE_*) for an image: 2x16 tiles near face-on, else Morton."""
+    """The library's pixel order (PHX_TILE_*) for an image: 4x8 tiles, centre first."""
     return lib().phx_default_pixel_order(C.byref(params))
 
 

@@ -91,9 +91,9 @@ def test_autotuner_and_stream_launch(gpu_snapshots):
     items = [_item(gpu_snapshots, "cfg1", "fp32", inclination=float(i)) for i in (10, 50, 120, 170)]
     with P.Batch(items, autotune=True, sample_stride=4) as b:
         t = b.tuning()
-        # 3 register caps x 3 refill periods, then the 4 other tile shapes at the best of those
-        assert t["ncand"] == 13 and len(t["candidates"]) == 13
-        assert sorted(c["tile_shape"] for c in t["candidates"][9:]) == [1, 2, 3, 4]
+        # 3 register caps x 3 refill periods, then the 5 other tile shapes at the best of those
+        assert t["ncand"] == 14 and len(t["candidates"]) == 14
+        assert sorted(c["tile_shape"] for c in t["candidates"][9:]) == [1, 2, 3, 4, 5]
         best = min(t["candidates"], key=lambda c: c["ms"])
         assert (t["blocks_per_sm"], t["period"], t["tile_shape"]) == (best["blocks_per_sm"], best["period"],
                                                                       best["tile_shape"])

@@ -65,14 +65,34 @@ def test_tile_schedules(built, shape, tw, th, wh):
         native.schedule_tiles(W, H, 9)
 
 
+@pytest.mark.parametrize("wh", [(1, 1), (13, 7), (64, 64), (96, 40), (512, 512)])
+def test_center_first_schedule(built, wh):
+    """4x8 tiles (j fastest inside one), nearest to the image centre first, ties in the tiles' Morton order."""
+    W, H = wh
+    tw, th = 4, 8
+    jobs = native.schedule_tiles(W, H, "center4x8")
+    assert np.array_equal(np.sort(jobs), np.arange(W * H))
+    nti, ntj = -(-W // tw), -(-H // th)
+
+    def d2(t):
+        ti, tj = divmod(int(t), ntj)
+        ci = 0.5 * (ti * tw + min(W, (ti + 1) * tw)) - 0.5 * W
+        cj = 0.5 * (tj * th + min(H, (tj + 1) * th)) - 0.5 * H
+        return ci * ci + cj * cj
+
+    want = []
+    for t in sorted(_schedule_reference_order(nti, ntj), key=d2):  # sorted() is stable
+        ti, tj = divmod(int(t), ntj)
+        want += [i * H + j for i in range(ti * tw, min(W, (ti + 1) * tw)) for j in range(tj * th, min(H, (tj + 1) * th))]
+    assert np.array_equal(jobs, np.array(want, dtype=np.int32))
+
+
 def test_default_pixel_order(built):
-    """2x16 tiles within about 41 degrees of the spin axis (|cos i| >= 0.75), Morton elsewhere."""
-    got = {i: native.default_pixel_order(native.make_params(inclination=i)) for i in (0, 10, 35, 41, 42, 60, 90, 120,
-                                                                                     138, 140, 163, 180)}
-    two, mort = native.TILE_SHAPES["2x16"], native.TILE_SHAPES["morton"]
-    assert got == {0: two, 10: two, 35: two, 41: two, 42: mort, 60: mort, 90: mort, 120: mort, 138: mort, 140: two,
-                   163: two, 180: two}
-    assert native.lib().phx_default_pixel_order(None) == mort
+    """Centre-first 4x8 tiles for every image."""
+    c = native.TILE_SHAPES["center4x8"]
+    for i in (0, 10, 35, 60, 90, 120, 163, 180):
+        assert native.default_pixel_order(native.make_params(inclination=i)) == c
+    assert native.lib().phx_default_pixel_order(None) == c
 
 
 def _read_host(dump, grid, spec, f64=True):
