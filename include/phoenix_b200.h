@@ -245,8 +245,9 @@ typedef struct {
 } PhxBatchOptions;
 
 /* Tile shapes: Morton (Z-order, 8x4-pixel warp tiles, the reference's host::jobs::schedule), or tiles of w x h pixels
- * (w along i, h along j; pixels j-fastest inside a tile), the tiles in Morton order of their coordinates, or for
- * PHX_TILE_CENTER_4X8 by the distance of their centre from the image centre, nearest first. */
+ * (w along i, h along j; pixels j-fastest inside a tile), the tiles in Morton order of their coordinates.
+ * PHX_TILE_CENTER_4X8: 4x8 tiles grouped in 32x32-pixel blocks, the blocks nearest the image centre first (ties in
+ * Morton order), the tiles of a block in Morton order. */
 enum {
   PHX_TILE_MORTON = 0,
   PHX_TILE_16X2 = 1,
@@ -257,11 +258,13 @@ enum {
   PHX_TILE_SHAPES = 6
 };
 /* The pixel order (PHX_TILE_*) for an image, which phx_render uses when it is given no job list and the serving loop
- * uses for every request: PHX_TILE_CENTER_4X8, for every image (the argument is not read, and may be NULL).  A
- * pixel's result does not depend on the order, but a launch ends when its last rays do: the longest rays (photon ring,
- * plunging orbits) sit near the image centre and the shortest at its edge, so centre-first tiles start the long rays
- * early and leave short ones for the end.  On B200, FP32 512^2 images of one snapshot, it ran 6-15 % faster than
- * Morton at every inclination tried (10-163 degrees). */
+ * uses for every request: PHX_TILE_CENTER_4X8 for images of up to 6 rays per lane of a full grid of the current
+ * device (SMs x 512 lanes; 148 SMs if no device can be queried: 454,656 pixels on B200), Morton for larger ones and
+ * for a NULL p.  A pixel's result does not depend on the order, but a launch ends when its last rays do: the longest
+ * rays (photon ring, plunging orbits) sit near the image centre and the shortest at its edge, so centre-first blocks
+ * start the long rays early and leave short ones for the end, which matters while an image is a few rays per lane.
+ * On B200, FP32: 512^2 images 6-12 % faster than Morton at 10, 60 and 163 degrees; a 1024^2 image 5 % slower (the
+ * jobs in flight then cover a thin ring instead of a compact patch of the image). */
 int phx_default_pixel_order(const PhxRenderParams* p);
 
 #define PHX_TUNE_MAX_CANDIDATES 16

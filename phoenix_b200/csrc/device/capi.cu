@@ -332,7 +332,18 @@ int phx_schedule_morton(int32_t W, int32_t H, int32_t* jobs) {
   });
 }
 
-int phx_default_pixel_order(const PhxRenderParams*) { return PHX_TILE_CENTER_4X8; }
+int phx_default_pixel_order(const PhxRenderParams* p) {
+  if (!p) return PHX_TILE_MORTON;
+  // lanes of a full grid of the single-image kernel on the current device (148 SMs x 512 if it cannot be queried)
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
+                                                cudaSuccess || sms < 1) {
+    cudaGetLastError();
+    sms = 148;
+  }
+  const long long lanes = (long long)sms * 512;
+  return (long long)p->img_width * p->img_height <= 6 * lanes ? PHX_TILE_CENTER_4X8 : PHX_TILE_MORTON;
+}
 
 int phx_schedule_tiles(int32_t W, int32_t H, int32_t shape, int32_t* jobs) {
   if (shape == PHX_TILE_MORTON) return phx_schedule_morton(W, H, jobs);
@@ -345,14 +356,26 @@ int phx_schedule_tiles(int32_t W, int32_t H, int32_t shape, int32_t* jobs) {
     std::vector<int32_t> tiles((size_t)nti * ntj);
     if (phx_schedule_morton(nti, ntj, tiles.data()) != PHX_OK) throw std::runtime_error(last_error());
     if (shape == PHX_TILE_CENTER_4X8) {
-      // tiles by the distance of their centre from the image centre (in pixels), nearest first; ties in Morton order
-      auto d2 = [&](int32_t t) {
-        const int32_t ti = t / ntj, tj = t % ntj;
-        const double ci = 0.5 * (ti * tw + std::min(W, (ti + 1) * tw)) - 0.5 * W;
-        const double cj = 0.5 * (tj * th + std::min(H, (tj + 1) * th)) - 0.5 * H;
+      // 32 x 32-pixel blocks by the distance of their centre from the image centre (in pixels), nearest first, ties
+      // in Morton order; inside a block its 4 x 8 tiles in Morton order (a stable sort of the Morton tile list by
+      // block rank)
+      constexpr int kB = 32;
+      const int32_t nbi = (W + kB - 1) / kB, nbj = (H + kB - 1) / kB;
+      std::vector<int32_t> blocks((size_t)nbi * nbj), rank((size_t)nbi * nbj);
+      if (phx_schedule_morton(nbi, nbj, blocks.data()) != PHX_OK) throw std::runtime_error(last_error());
+      auto d2 = [&](int32_t b) {
+        const int32_t bi = b / nbj, bj = b % nbj;
+        const double ci = 0.5 * (bi * kB + std::min(W, (bi + 1) * kB)) - 0.5 * W;
+        const double cj = 0.5 * (bj * kB + std::min(H, (bj + 1) * kB)) - 0.5 * H;
         return ci * ci + cj * cj;
       };
-      std::stable_sort(tiles.begin(), tiles.end(), [&](int32_t a, int32_t b) { return d2(a) < d2(b); });
+      std::stable_sort(blocks.begin(), blocks.end(), [&](int32_t a, int32_t b) { return d2(a) < d2(b); });
+      for (size_t r = 0; r < blocks.size(); r++) rank[blocks[r]] = (int32_t)r;
+      auto block_of = [&](int32_t t) {
+        const int32_t ti = t / ntj, tj = t % ntj;
+        return rank[(size_t)(ti * tw / kB) * nbj + tj * th / kB];
+      };
+      std::stable_sort(tiles.begin(), tiles.end(), [&](int32_t a, int32_t b) { return block_of(a) < block_of(b); });
     }
     size_t n = 0;
     for (const int32_t t : tiles) {

@@ -65,34 +65,41 @@ def test_tile_schedules(built, shape, tw, th, wh):
         native.schedule_tiles(W, H, 9)
 
 
-@pytest.mark.parametrize("wh", [(1, 1), (13, 7), (64, 64), (96, 40), (512, 512)])
+@pytest.mark.parametrize("wh", [(1, 1), (13, 7), (64, 64), (96, 40), (100, 260), (512, 512)])
 def test_center_first_schedule(built, wh):
-    """4x8 tiles (j fastest inside one), nearest to the image centre first, ties in the tiles' Morton order."""
+    """4x8 tiles in 32x32-pixel blocks: blocks nearest the image centre first (ties in Morton order), the tiles of a
+    block in Morton order, pixels j-fastest inside a tile."""
     W, H = wh
-    tw, th = 4, 8
+    tw, th, B = 4, 8, 32
     jobs = native.schedule_tiles(W, H, "center4x8")
     assert np.array_equal(np.sort(jobs), np.arange(W * H))
     nti, ntj = -(-W // tw), -(-H // th)
+    nbi, nbj = -(-W // B), -(-H // B)
 
-    def d2(t):
-        ti, tj = divmod(int(t), ntj)
-        ci = 0.5 * (ti * tw + min(W, (ti + 1) * tw)) - 0.5 * W
-        cj = 0.5 * (tj * th + min(H, (tj + 1) * th)) - 0.5 * H
+    def d2(b):
+        bi, bj = divmod(int(b), nbj)
+        ci = 0.5 * (bi * B + min(W, (bi + 1) * B)) - 0.5 * W
+        cj = 0.5 * (bj * B + min(H, (bj + 1) * B)) - 0.5 * H
         return ci * ci + cj * cj
 
+    rank = {int(b): r for r, b in enumerate(sorted(_schedule_reference_order(nbi, nbj), key=d2))}  # stable
+    tiles = sorted(_schedule_reference_order(nti, ntj),
+                   key=lambda t: rank[(int(t) // ntj) * tw // B * nbj + (int(t) % ntj) * th // B])
     want = []
-    for t in sorted(_schedule_reference_order(nti, ntj), key=d2):  # sorted() is stable
+    for t in tiles:
         ti, tj = divmod(int(t), ntj)
         want += [i * H + j for i in range(ti * tw, min(W, (ti + 1) * tw)) for j in range(tj * th, min(H, (tj + 1) * th))]
     assert np.array_equal(jobs, np.array(want, dtype=np.int32))
 
 
 def test_default_pixel_order(built):
-    """Centre-first 4x8 tiles for every image."""
-    c = native.TILE_SHAPES["center4x8"]
-    for i in (0, 10, 35, 60, 90, 120, 163, 180):
-        assert native.default_pixel_order(native.make_params(inclination=i)) == c
-    assert native.lib().phx_default_pixel_order(None) == c
+    """Centre-first blocks up to 6 rays per lane of a full grid (148 SMs x 512 lanes here: no GPU), Morton beyond."""
+    c, m = native.TILE_SHAPES["center4x8"], native.TILE_SHAPES["morton"]
+    lanes = 148 * 512
+    for side, want in ((64, c), (512, c), (674, c), (675, m), (1024, m), (2048, m)):
+        assert (side * side <= 6 * lanes) == (want == c)
+        assert native.default_pixel_order(native.make_params(img=side)) == want, side
+    assert native.lib().phx_default_pixel_order(None) == m
 
 
 def _read_host(dump, grid, spec, f64=True):
