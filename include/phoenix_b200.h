@@ -99,7 +99,7 @@ typedef struct {
   double r_fp64;       /* unused (kept for layout; the mixed mode integrates every step in FP64) */
   double tau_fp64;     /* mixed: FP64 segment operator where h max|K| exceeds this (<= 0: default 0.1) */
   int32_t block;       /* unused (the block shape follows blocks_per_sm; PhxRenderInfo.block reports it) */
-  int32_t period;      /* march passes between lane refills, 0 = default (64) */
+  int32_t period;      /* march passes between lane refills, 0 = default (256) */
   int32_t blocks_per_sm; /* register-cap variant, as resident warps per SM / 4 (1: up to 255 registers in 128-thread
                             blocks; 3: 168 registers, 4: 128, as one 384 / 512-thread block per SM when the job list
                             fills every SM, else as 128-thread blocks); 0 = default (FP32 4; mixed 4 with one frequency, else 3;

@@ -186,7 +186,7 @@ void run_setup(PhxBatch* b) {
 
 void autotune(PhxBatch* b) {
   std::vector<phx::QueueShape> cand;
-  const int periods[] = {16, 32, 64};
+  const int periods[] = {32, 64, 128};
   if (b->precision == PHX_PREC_FP32 && b->nf_slots <= 4) {
     for (int bps : {3, 4, 1})
       for (int per : periods) cand.push_back({bps, per});
@@ -373,7 +373,7 @@ PhxBatch* create_batch(const PhxBatchItem* items, int32_t nitems, const PhxBatch
   ck(cudaEventCreate(&b->e1), "cudaEventCreate");
   b->shape = {o.blocks_per_sm > 0 ? o.blocks_per_sm
                                   : (b->precision == PHX_PREC_FP32 ? 4 : b->precision == PHX_PREC_MIXED ? 3 : 1),
-             o.period > 0 ? o.period : phx::kDefaultPeriod};
+             o.period > 0 ? o.period : phx::kDefaultQueuePeriod};
   run_setup(b.get());
   if (o.autotune && b->ntrial > 0) autotune(b.get());
   capture(b.get());

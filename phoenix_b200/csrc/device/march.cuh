@@ -115,8 +115,13 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
   }
 }
 
-// Default march passes between lane refills (measured best on B200 for the single-image and queue kernels).
-constexpr int kDefaultPeriod = 64;
+// Default march passes between lane refills.  Single-image kernel (measured on B200, 3 x 512^2 bench images, FP32,
+// centre-first job lists, two runs each): 64 passes 248 ms, 128 245, 192 244, 256 242; mixed 400 / 395 / 393 ms at
+// 64 / 128 / 256.  A longer period leaves finished lanes idle longer but refills more lanes per warp at once, and the
+// FP64 camera set-up of those lanes then runs in one pass of the warp instead of several.  Queue kernel (batches,
+// serving; autotuned for batches): 64.
+constexpr int kDefaultPeriod = 256;
+constexpr int kDefaultQueuePeriod = 64;
 
 // Launch entry per (mode, prim type): picks the frequency-slot instantiation and the launch shape.
 struct LaunchShape {

@@ -583,7 +583,7 @@ PhxServer* create_server(PhxSnapshot* const* snaps, int32_t nsnaps, const PhxSer
   if ((o.max_tiles & (o.max_tiles - 1)) != 0) throw std::invalid_argument("max_tiles must be a power of two");
   if (o.max_freqs <= 0) o.max_freqs = 4;
   if (o.max_freqs > 4 && o.precision != PHX_PREC_FP32) throw std::invalid_argument("more than 4 frequencies: FP32 only");
-  if (o.period <= 0) o.period = phx::kDefaultPeriod;
+  if (o.period <= 0) o.period = phx::kDefaultQueuePeriod;
   if (o.idle_ns <= 0) o.idle_ns = 2000;
   if (o.idle_limit <= 0) o.idle_limit = 5000000;
   if (o.linger_ms < 0) o.linger_ms = 0;
@@ -656,7 +656,7 @@ void phx_default_server_options(PhxServerOptions* o) {
   o->precision = PHX_PREC_FP32;
   o->max_freqs = 4;
   o->tile_rays = 32;
-  o->period = phx::kDefaultPeriod;
+  o->period = phx::kDefaultQueuePeriod;
   o->blocks_per_sm = 0;
   o->max_items = 4096;
   o->max_tiles = 1 << 22;

@@ -133,7 +133,7 @@ def test_results_independent_of_scheduling(gpu_snapshots, bps):
     (separate compilations), so across them the images agree to FP32 rounding."""
     kw = case_params("cfg1")
     base, _ = gpu_snapshots["cfg1"].render(P.make_params(precision="fp32", blocks_per_sm=bps, period=1, **kw))
-    for period in (4, 16, 64):
+    for period in (4, 16, 64, 256):
         other, _ = gpu_snapshots["cfg1"].render(P.make_params(precision="fp32", blocks_per_sm=bps, period=period, **kw))
         assert np.array_equal(base, other), (bps, period)
     default, _ = gpu_snapshots["cfg1"].render(P.make_params(precision="fp32", **kw))
