@@ -186,7 +186,7 @@ void run_setup(PhxBatch* b) {
 
 void autotune(PhxBatch* b) {
   std::vector<phx::QueueShape> cand;
-  const int periods[] = {32, 64, 128};
+  const int periods[] = {64, 128, 256};
   if (b->precision == PHX_PREC_FP32 && b->nf_slots <= 4) {
     for (int bps : {3, 4, 1})
       for (int per : periods) cand.push_back({bps, per});
