@@ -99,11 +99,14 @@ typedef struct {
   double r_fp64;       /* unused (kept for layout; the mixed mode integrates every step in FP64) */
   double tau_fp64;     /* mixed: FP64 segment operator where h max|K| exceeds this (<= 0: default 0.1) */
   int32_t block;       /* unused (the block shape follows blocks_per_sm; PhxRenderInfo.block reports it) */
-  int32_t period;      /* march passes between lane refills, 0 = default (256) */
+  int32_t period;      /* march passes after which a warp refills its finished lanes even if others still run,
+                          0 = default (2^20: longer than any ray, so a warp refills when it is empty) */
   int32_t blocks_per_sm; /* register-cap variant, as resident warps per SM / 4 (1: up to 255 registers in 128-thread
                             blocks; 3: 168 registers, 4: 128, as one 384 / 512-thread block per SM when the job list
                             fills every SM, else as 128-thread blocks); 0 = default (FP32 4; mixed 4 with one frequency, else 3;
                             FP64 1) */
+  int32_t refill_lanes; /* a warp takes new jobs early, before the period ends, once this many of its 32 lanes have
+                           finished (checked every 64 passes); 1..32, 0 = default (32: when the warp is empty) */
 } PhxRenderParams;
 
 /* What a render reports (a superset of the reference's device::Info, src/device/kernel.cuh:23-30). */
@@ -233,15 +236,18 @@ typedef struct {
   int32_t tile_rays;       /* rays per queue tile, 0 = 32 */
   int32_t blocks_per_sm;   /* register-cap variant (FP32: 1, 3, 4; mixed 1, 3, and 4 with one frequency slot),
                               0 = default (FP32 4; mixed 4 with one slot, else 3; FP64 1) or autotuned */
-  int32_t period;          /* march passes between lane refills, 0 = default 64 or autotuned */
-  int32_t autotune;        /* nonzero: time every (blocks_per_sm, period) candidate on a sample of the batch's tiles
-                              at creation, then every tile shape at the fastest of them, and keep the fastest */
+  int32_t period;          /* march passes after which a warp claims slots for its finished lanes even if others still
+                              run, 0 = default (2^20) or autotuned */
+  int32_t autotune;        /* nonzero: time every (blocks_per_sm, refill policy) candidate on a sample of the batch's
+                              tiles at creation, then every tile shape at the fastest of them, and keep the fastest */
   int32_t sample_stride;   /* autotune sample: every n-th tile, 0 = 16 */
   int32_t keep_order;      /* nonzero: tiles in item order; 0: the largest images' tiles first */
   int32_t tile_shape;      /* pixel order of the items without a job list, i.e. the shape of the pixel tile a warp's
                               32 consecutive rays cover: PHX_TILE_* (0 = Morton, the reference's schedule) */
   int32_t lane_setup;      /* nonzero: each lane sets up the camera ray it takes (no start-state buffer); 0: a ray-setup
                               kernel sets up every job at full SIMD width before the queue kernel, in the same graph */
+  int32_t refill_lanes;    /* a warp claims new slots early once this many of its lanes have finished (checked every 64
+                              passes); 1..32, 0 = default (32: when the warp is empty) or autotuned */
 } PhxBatchOptions;
 
 /* Tile shapes: Morton (Z-order, 8x4-pixel warp tiles, the reference's host::jobs::schedule), or tiles of w x h pixels
@@ -278,6 +284,8 @@ typedef struct {
   int32_t cand_tile_shape[PHX_TUNE_MAX_CANDIDATES];
   int64_t nitems, ntiles, nrays;
   int64_t device_bytes;  /* device memory the batch holds (tables, job lists, results) */
+  int32_t refill_lanes;  /* refill threshold in use */
+  int32_t cand_refill_lanes[PHX_TUNE_MAX_CANDIDATES];
 } PhxBatchTuning;
 
 void phx_default_batch_options(PhxBatchOptions* o);
@@ -325,7 +333,7 @@ typedef struct {
   int32_t precision;      /* PHX_PREC_*, shared by every request */
   int32_t max_freqs;      /* frequency slots per request (1 or 4; FP32 also up to 32), default 4 */
   int32_t tile_rays;      /* rays per queue tile, default 32 */
-  int32_t period;         /* march passes between lane refills, default 64 */
+  int32_t period;         /* march passes after which a warp claims slots for its finished lanes, default 2^20 */
   int32_t blocks_per_sm;  /* register-cap variant, 0 = default (FP32 4; mixed 4 with one slot, else 3; FP64 1) */
   int32_t max_items;      /* requests per run of the kernel before the queue is recycled, default 4096 */
   int64_t max_tiles;      /* tiles per run of the kernel, a power of two, default 2^22 */
@@ -337,6 +345,7 @@ typedef struct {
   int64_t backlog_rays;   /* published but unclaimed rays kept in the queue, 0 = half a grid-load of lanes */
   int64_t small_rays;     /* requests of at most this many rays enter the queue whole, ahead of the large ones'
                              remaining tiles (default 65536, a 256^2 image) */
+  int32_t refill_lanes;   /* a warp claims new slots early once this many of its lanes have finished, default 32 */
 } PhxServerOptions;
 
 typedef struct {

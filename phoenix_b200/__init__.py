@@ -133,7 +133,7 @@ class Batch:
     (snapshot, params, jobs) tuples."""
 
     def __init__(self, items, tile_rays=32, blocks_per_sm=0, period=0, autotune=False, sample_stride=16,
-                 keep_order=False, tile_shape=0, lane_setup=False):
+                 keep_order=False, tile_shape=0, lane_setup=False, refill_lanes=0):
         L = native.lib()
         n = len(items)
         arr = (native.PhxBatchItem * n)()
@@ -150,7 +150,7 @@ class Batch:
                 arr[k].jobs, arr[k].njobs = j.ctypes.data, j.size
             self.params.append(p)
         o = native.PhxBatchOptions(tile_rays, blocks_per_sm, period, 1 if autotune else 0, sample_stride,
-                                   1 if keep_order else 0, tile_shape, 1 if lane_setup else 0)
+                                   1 if keep_order else 0, tile_shape, 1 if lane_setup else 0, refill_lanes)
         h = C.c_void_p()
         native.check(L.phx_batch_create(arr, n, C.byref(o), C.byref(h)))
         self._h = h

@@ -186,18 +186,19 @@ void run_setup(PhxBatch* b) {
 
 void autotune(PhxBatch* b) {
   std::vector<phx::QueueShape> cand;
-  const int periods[] = {64, 128, 256};
+  // refill policies: the finished lanes every 128 passes; a warp with 24 finished lanes; a warp with all 32 finished
+  const int policies[3][2] = {{128, 1}, {phx::kDefaultQueuePeriod, 24}, {phx::kDefaultQueuePeriod, 32}};
+  auto add = [&](int bps) {
+    for (const auto& pol : policies) cand.push_back({bps, pol[0], pol[1]});
+  };
   if (b->precision == PHX_PREC_FP32 && b->nf_slots <= 4) {
-    for (int bps : {3, 4, 1})
-      for (int per : periods) cand.push_back({bps, per});
+    for (int bps : {3, 4, 1}) add(bps);
   } else if (b->precision == PHX_PREC_MIXED && b->nf_slots == 1) {
-    for (int bps : {3, 4, 1})
-      for (int per : periods) cand.push_back({bps, per});
+    for (int bps : {3, 4, 1}) add(bps);
   } else if (b->precision == PHX_PREC_MIXED) {
-    for (int bps : {3, 1})
-      for (int per : periods) cand.push_back({bps, per});
+    for (int bps : {3, 1}) add(bps);
   } else {
-    for (int per : periods) cand.push_back({0, per});
+    add(0);
   }
   // load every variant once (an empty queue: the kernel leaves at its first refill)
   phx::LaunchShape ls;
@@ -207,11 +208,12 @@ void autotune(PhxBatch* b) {
     if (nc >= PHX_TUNE_MAX_CANDIDATES) return;
     b->tuning.cand_blocks_per_sm[nc] = q.blocks_per_sm;
     b->tuning.cand_period[nc] = q.period;
+    b->tuning.cand_refill_lanes[nc] = q.refill_lanes;
     b->tuning.cand_tile_shape[nc] = shape;
     b->tuning.cand_ms[nc] = ms;
     nc++;
   };
-  // stage 1: register cap x refill period, in the current pixel order
+  // stage 1: register cap x refill policy, in the current pixel order
   const int shape0 = b->tile_shape;
   float best = 1e30f;
   for (size_t c = 0; c < cand.size(); c++) {
@@ -286,6 +288,7 @@ PhxBatch* create_batch(const PhxBatchItem* items, int32_t nitems, const PhxBatch
     throw std::invalid_argument("batches with more than 4 frequencies per image are FP32 only");
   // job lists (validated) and result offsets
   if (o.tile_shape < 0 || o.tile_shape >= PHX_TILE_SHAPES) throw std::invalid_argument("unknown tile_shape");
+  if (o.refill_lanes < 0 || o.refill_lanes > 32) throw std::invalid_argument("refill_lanes must be in 0..32");
   b->tile_shape = o.tile_shape;
   std::vector<int32_t> all_jobs;
   std::vector<size_t>& job_off = b->job_off;
@@ -371,14 +374,16 @@ PhxBatch* create_batch(const PhxBatchItem* items, int32_t nitems, const PhxBatch
   ck(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "cudaStreamCreate");
   ck(cudaEventCreate(&b->e0), "cudaEventCreate");
   ck(cudaEventCreate(&b->e1), "cudaEventCreate");
-  b->shape = {o.blocks_per_sm > 0 ? o.blocks_per_sm
-                                  : (b->precision == PHX_PREC_FP32 ? 4 : b->precision == PHX_PREC_MIXED ? 3 : 1),
-             o.period > 0 ? o.period : phx::kDefaultQueuePeriod};
+  b->shape = {o.blocks_per_sm > 0
+                  ? o.blocks_per_sm
+                  : (b->precision == PHX_PREC_FP32 ? 4 : b->precision == PHX_PREC_MIXED ? (b->nf_slots == 1 ? 4 : 3) : 1),
+              o.period > 0 ? o.period : phx::kDefaultQueuePeriod, o.refill_lanes > 0 ? o.refill_lanes : 32};
   run_setup(b.get());
   if (o.autotune && b->ntrial > 0) autotune(b.get());
   capture(b.get());
   b->tuning.blocks_per_sm = b->shape.blocks_per_sm;
   b->tuning.period = b->shape.period;
+  b->tuning.refill_lanes = b->shape.refill_lanes;
   b->tuning.tile_rays = b->tile_rays;
   b->tuning.tile_shape = b->tile_shape;
   b->tuning.grid = b->lshape.grid;

@@ -40,6 +40,7 @@ cudaError_t launch_mode(PhxSnapshot* s, const PhxRenderParams& p, const typename
   A.pixstats = d_pixstats;
   A.counters = reinterpret_cast<unsigned long long*>(d_counters);
   A.period = p.period > 0 ? p.period : phx::kDefaultPeriod;  // passes between lane refills (measured best on B200)
+  A.refill_lanes = p.refill_lanes > 0 ? p.refill_lanes : 32;
   return phx::launch_march<M, PT>(A, s->sms, p.blocks_per_sm, st, shape);
 }
 

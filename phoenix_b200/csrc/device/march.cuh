@@ -40,6 +40,7 @@ struct MarchArgs {
   int32_t* pixstats;
   unsigned long long* counters;
   int32_t period;
+  int32_t refill_lanes;  // finished lanes at which a warp refills before its period ends (checked every 64 passes)
 };
 
 __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
@@ -97,6 +98,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
           rays++;
         }
       }
+      // a warp with refill_lanes finished lanes refills at once instead of at the end of the period
+      if ((it & 63) == 63 && __popc(__ballot_sync(0xffffffffu, !live)) >= A.refill_lanes) break;
     }
   }
   const unsigned long long wsteps = warp_sum_u64(steps), wnplasma = warp_sum_u64(nplasma), wbad = warp_sum_u64(bad),
@@ -115,13 +118,17 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
   }
 }
 
-// Default march passes between lane refills.  Single-image kernel (measured on B200, 3 x 512^2 bench images, FP32,
-// centre-first job lists, two runs each): 64 passes 248 ms, 128 245, 192 244, 256 242; mixed 400 / 395 / 393 ms at
-// 64 / 128 / 256.  A longer period leaves finished lanes idle longer but refills more lanes per warp at once, and the
-// FP64 camera set-up of those lanes then runs in one pass of the warp instead of several.  Queue kernel (batches,
-// serving; autotuned for batches): 64.
-constexpr int kDefaultPeriod = 256;
-constexpr int kDefaultQueuePeriod = 64;
+// Refill policy of the single-image kernel: a warp takes new jobs when all its lanes have finished (refill_lanes 32,
+// checked every 64 passes), or at the end of a period, by default longer than any ray.  Measured on B200 (FP32,
+// centre-first job lists; ms for the 3 x 512^2 bench images / one 1024^2 image of 3 frequencies): a refill of the
+// finished lanes every 64 passes 247 / 480, every 256 243 / 433, every 4096 233 / 370; whole-warp refill 231 / 363;
+// refill once 24 lanes have finished 237 / 378, 8 lanes 242 / 433.  Lanes refilled one or two at a time start their
+// rays in a different phase than their neighbours (far from the hole, no plasma, long steps): the warp then pays
+// for both phases' code at every pass, which costs more than the lanes a whole-warp refill leaves idle behind the
+// warp's longest ray; rays that start together from neighbouring pixels stay in step.  The queue kernel (batches,
+// serving) uses the same policy by default; batches autotune it.
+constexpr int kDefaultPeriod = 1 << 20;
+constexpr int kDefaultQueuePeriod = 1 << 20;
 
 // Launch entry per (mode, prim type): picks the frequency-slot instantiation and the launch shape.
 struct LaunchShape {

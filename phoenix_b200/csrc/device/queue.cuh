@@ -69,6 +69,7 @@ struct QueueArgs {
   unsigned tile_mask;            // ring capacity - 1 (a power of two)
   int32_t tile_rays;
   int32_t period;
+  int32_t refill_lanes;          // finished lanes at which a warp claims new slots before its period ends
   int32_t idle_ns;               // sleep between polls of an idle warp; 0: leave once the published tiles are drained
   long long idle_limit;          // polls before an idle warp gives up (status word set)
 };
@@ -175,6 +176,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
           }
         }
       }
+      // a warp with refill_lanes finished lanes claims new slots at once instead of at the end of the period
+      if ((it & 63) == 63 && __popc(__ballot_sync(kFull, !live)) >= A.refill_lanes) break;
     }
   }
   steps = warp_sum_u64(steps);
@@ -218,6 +221,7 @@ cudaError_t launch_ray_setup(const ItemDesc<typename Policy<M>::R, PT>& item, lo
 struct QueueShape {
   int blocks_per_sm;  // register-cap variant: 1, 3 or 4 (FP32); mixed 1, 3 (4 with one slot); FP64 1; 0 = default
   int period;
+  int refill_lanes;   // 1..32 (0: 32, when the warp is empty)
 };
 
 // Default register-cap variant (measured on B200): FP32 128 registers (16 warps per SM); mixed 128 with one frequency

@@ -8,7 +8,7 @@
 namespace phx {
 
 template <Mode M, class PT, int NF, int kQueueBlock, int kMinBlocks>
-cudaError_t launch_queue_mb(const QueueArgs<typename Policy<M>::R, PT>& args, int sms, int period, long long max_rays,
+cudaError_t launch_queue_mb(const QueueArgs<typename Policy<M>::R, PT>& args, int sms, QueueShape qs, long long max_rays,
                             cudaStream_t stream, LaunchShape* shape) {
   auto kern = k_queue<M, PT, NF, kQueueBlock, kMinBlocks>;
   // the rays' transfer records (shared-memory kernels; 0 otherwise)
@@ -33,7 +33,8 @@ cudaError_t launch_queue_mb(const QueueArgs<typename Policy<M>::R, PT>& args, in
   shape->local_bytes = (int)fa.localSizeBytes;
   shape->blocks_per_sm = bpsm;
   QueueArgs<typename Policy<M>::R, PT> a = args;
-  a.period = period > 0 ? period : 32;
+  a.period = qs.period > 0 ? qs.period : 32;
+  a.refill_lanes = qs.refill_lanes > 0 ? qs.refill_lanes : 32;
   kern<<<(unsigned)grid, kQueueBlock, smem, stream>>>(a);
   return cudaGetLastError();
 }
@@ -46,21 +47,21 @@ template <Mode M, class PT, int NF>
 cudaError_t launch_queue_nf(const QueueArgs<typename Policy<M>::R, PT>& args, int sms, QueueShape q,
                             long long max_rays, cudaStream_t stream, LaunchShape* shape) {
   if constexpr (M == Mode::kFP64 || NF > 4) {
-    return launch_queue_mb<M, PT, NF, 128, 1>(args, sms, q.period, max_rays, stream, shape);
+    return launch_queue_mb<M, PT, NF, 128, 1>(args, sms, q, max_rays, stream, shape);
   } else {
     const int bps = q.blocks_per_sm > 0 ? q.blocks_per_sm : default_queue_blocks_per_sm<M, NF>();
     const bool whole = max_rays <= 0 || max_rays >= (long long)sms * 128 * bps;
     if (bps == 3) {
-      return whole ? launch_queue_mb<M, PT, NF, 384, 1>(args, sms, q.period, max_rays, stream, shape)
-                   : launch_queue_mb<M, PT, NF, 128, 3>(args, sms, q.period, max_rays, stream, shape);
+      return whole ? launch_queue_mb<M, PT, NF, 384, 1>(args, sms, q, max_rays, stream, shape)
+                   : launch_queue_mb<M, PT, NF, 128, 3>(args, sms, q, max_rays, stream, shape);
     }
     if constexpr (M == Mode::kFP32 || (M == Mode::kMixed && NF == 1)) {
       if (bps == 4) {
-        return whole ? launch_queue_mb<M, PT, NF, 512, 1>(args, sms, q.period, max_rays, stream, shape)
-                     : launch_queue_mb<M, PT, NF, 128, 4>(args, sms, q.period, max_rays, stream, shape);
+        return whole ? launch_queue_mb<M, PT, NF, 512, 1>(args, sms, q, max_rays, stream, shape)
+                     : launch_queue_mb<M, PT, NF, 128, 4>(args, sms, q, max_rays, stream, shape);
       }
     }
-    return launch_queue_mb<M, PT, NF, 128, 1>(args, sms, q.period, max_rays, stream, shape);
+    return launch_queue_mb<M, PT, NF, 128, 1>(args, sms, q, max_rays, stream, shape);
   }
 }
 

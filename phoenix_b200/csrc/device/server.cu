@@ -201,7 +201,7 @@ void bind_mode(PhxServer* s) {
     A.period = self->o.period;
     A.idle_ns = self->o.idle_ns;
     A.idle_limit = self->o.idle_limit;
-    phx::QueueShape q{self->o.blocks_per_sm, self->o.period};
+    phx::QueueShape q{self->o.blocks_per_sm, self->o.period, self->o.refill_lanes};
     return phx::launch_queue<M, PT>(A, self->nf_slots, self->sms, q, 0, st, ls);
   };
 }
@@ -584,6 +584,8 @@ PhxServer* create_server(PhxSnapshot* const* snaps, int32_t nsnaps, const PhxSer
   if (o.max_freqs <= 0) o.max_freqs = 4;
   if (o.max_freqs > 4 && o.precision != PHX_PREC_FP32) throw std::invalid_argument("more than 4 frequencies: FP32 only");
   if (o.period <= 0) o.period = phx::kDefaultQueuePeriod;
+  if (o.refill_lanes < 0 || o.refill_lanes > 32) throw std::invalid_argument("refill_lanes must be in 0..32");
+  if (o.refill_lanes == 0) o.refill_lanes = 32;
   if (o.idle_ns <= 0) o.idle_ns = 2000;
   if (o.idle_limit <= 0) o.idle_limit = 5000000;
   if (o.linger_ms < 0) o.linger_ms = 0;
@@ -657,6 +659,7 @@ void phx_default_server_options(PhxServerOptions* o) {
   o->max_freqs = 4;
   o->tile_rays = 32;
   o->period = phx::kDefaultQueuePeriod;
+  o->refill_lanes = 32;
   o->blocks_per_sm = 0;
   o->max_items = 4096;
   o->max_tiles = 1 << 22;

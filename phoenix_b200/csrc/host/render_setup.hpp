@@ -38,6 +38,7 @@ inline void check_params(const PhxRenderParams& p) {
   if (!(p.beta_c > 0.0)) bad("beta_c must be > 0");
   if (!(p.mass > 0.0) || !(p.distance > 0.0) || !(p.m_unit > 0.0)) bad("mass, distance and m_unit must be > 0");
   if (p.precision < PHX_PREC_FP32 || p.precision > PHX_PREC_MIXED) bad("unknown precision mode");
+  if (p.refill_lanes < 0 || p.refill_lanes > 32) bad("refill_lanes must be in 0..32");
 }
 
 // Integration limits and step-size constants of a geodesic in precision G (the reference's FP32 / FP64 thresholds,

@@ -71,7 +71,7 @@ class PhxRenderParams(C.Structure):
         ("m_unit", C.c_double), ("r_low", C.c_double), ("r_high", C.c_double), ("beta_c", C.c_double),
         ("sigma_cut", C.c_double), ("thetae_min", C.c_double), ("thetae_max", C.c_double), ("rt_outer", C.c_double),
         ("precision", C.c_int32), ("r_fp64", C.c_double), ("tau_fp64", C.c_double),
-        ("block", C.c_int32), ("period", C.c_int32), ("blocks_per_sm", C.c_int32),
+        ("block", C.c_int32), ("period", C.c_int32), ("blocks_per_sm", C.c_int32), ("refill_lanes", C.c_int32),
     ]
 
 
@@ -96,7 +96,7 @@ class PhxBatchItem(C.Structure):
 class PhxBatchOptions(C.Structure):
     _fields_ = [("tile_rays", C.c_int32), ("blocks_per_sm", C.c_int32), ("period", C.c_int32),
                 ("autotune", C.c_int32), ("sample_stride", C.c_int32), ("keep_order", C.c_int32),
-                ("tile_shape", C.c_int32), ("lane_setup", C.c_int32)]
+                ("tile_shape", C.c_int32), ("lane_setup", C.c_int32), ("refill_lanes", C.c_int32)]
 
 
 class PhxBatchTuning(C.Structure):
@@ -107,13 +107,15 @@ class PhxBatchTuning(C.Structure):
         ("cand_period", C.c_int32 * TUNE_MAX_CANDIDATES), ("cand_ms", C.c_double * TUNE_MAX_CANDIDATES),
         ("tile_shape", C.c_int32), ("cand_tile_shape", C.c_int32 * TUNE_MAX_CANDIDATES),
         ("nitems", C.c_int64), ("ntiles", C.c_int64), ("nrays", C.c_int64), ("device_bytes", C.c_int64),
+        ("refill_lanes", C.c_int32), ("cand_refill_lanes", C.c_int32 * TUNE_MAX_CANDIDATES),
     ]
 
     def as_dict(self):
         n = self.ncand
         d = {name: getattr(self, name) for name, _ in self._fields_ if not name.startswith("cand_")}
         d["candidates"] = [dict(blocks_per_sm=self.cand_blocks_per_sm[i], period=self.cand_period[i],
-                                tile_shape=self.cand_tile_shape[i], ms=self.cand_ms[i]) for i in range(n)]
+                                refill_lanes=self.cand_refill_lanes[i], tile_shape=self.cand_tile_shape[i],
+                                ms=self.cand_ms[i]) for i in range(n)]
         return d
 
 
@@ -138,6 +140,7 @@ class PhxServerOptions(C.Structure):
         ("tile_rays", C.c_int32), ("period", C.c_int32), ("blocks_per_sm", C.c_int32), ("max_items", C.c_int32),
         ("max_tiles", C.c_int64), ("idle_ns", C.c_int32), ("idle_limit", C.c_int64), ("linger_ms", C.c_double),
         ("poll_us", C.c_int32), ("publish_chunk", C.c_int32), ("backlog_rays", C.c_int64), ("small_rays", C.c_int64),
+        ("refill_lanes", C.c_int32),
     ]
 
 

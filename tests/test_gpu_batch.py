@@ -45,6 +45,25 @@ def test_batch_items_match_oracle(gpu_snapshots, oracle_results, precision):
             assert abs(info["steps"] - int(st_ref[..., 0].sum())) <= 0.002 * st_ref[..., 0].sum(), name
 
 
+def test_result_independent_of_the_refill_policy(gpu_snapshots):
+    """Claiming slots for finished lanes every few passes, once a part of the warp has finished, or only when the whole
+    warp has: the same images bit for bit (only which lanes run which rays, and when, changes)."""
+    items = [_item(gpu_snapshots, n, "fp32") for n in ("thick", "cfg1", "edge")]
+    out = []
+    for period, refill in ((16, 1), (1 << 20, 24), (1 << 20, 32), (0, 0)):
+        with P.Batch(items, blocks_per_sm=4, period=period, refill_lanes=refill) as b:
+            b.run()
+            out.append([b.result(k)[0] for k in range(len(items))])
+            if (period, refill) == (0, 0):
+                t = b.tuning()
+                assert (t["period"], t["refill_lanes"]) == (1 << 20, 32)
+    for other in out[1:]:
+        for a, c in zip(out[0], other):
+            assert np.array_equal(a, c)
+    with pytest.raises(P.PhxError, match="refill_lanes"):
+        P.Batch(items, refill_lanes=33)
+
+
 def test_result_independent_of_the_mix(gpu_snapshots):
     """An image rendered alone and in a batch with other images (other snapshots, cameras, sizes) is bit-identical:
     a ray's arithmetic does not depend on its lane, warp or the rays around it."""

@@ -129,13 +129,14 @@ def test_frequencies_are_independent(gpu_snapshots):
 @pytest.mark.parametrize("bps", [0, 1, 4])
 def test_results_independent_of_scheduling(gpu_snapshots, bps):
     """A ray's arithmetic does not depend on which lane, warp or refill round runs it: for one compiled variant the
-    image is bit-identical whatever the refill period.  Variants compiled for other register caps round differently
+    image is bit-identical whatever the refill period or threshold.  Variants compiled for other register caps round differently
     (separate compilations), so across them the images agree to FP32 rounding."""
     kw = case_params("cfg1")
     base, _ = gpu_snapshots["cfg1"].render(P.make_params(precision="fp32", blocks_per_sm=bps, period=1, **kw))
-    for period in (4, 16, 64, 256):
-        other, _ = gpu_snapshots["cfg1"].render(P.make_params(precision="fp32", blocks_per_sm=bps, period=period, **kw))
-        assert np.array_equal(base, other), (bps, period)
+    for period, refill in ((4, 0), (16, 0), (64, 1), (256, 8), (1 << 20, 24), (1 << 20, 32)):
+        other, _ = gpu_snapshots["cfg1"].render(P.make_params(precision="fp32", blocks_per_sm=bps, period=period,
+                                                              refill_lanes=refill, **kw))
+        assert np.array_equal(base, other), (bps, period, refill)
     default, _ = gpu_snapshots["cfg1"].render(P.make_params(precision="fp32", **kw))
     l1 = np.abs(default[..., :4] - base[..., :4]).sum() / np.abs(base[..., :4]).sum()
     assert l1 <= 1e-5, l1
