@@ -318,7 +318,8 @@ def run_batch(args):
 
 def run_batch_small(args):
     """A small FP32 batch (the first N images of the sweep, all at 256^2): one graph launch per step, for profiling
-    the queue kernel on a case that ncu can capture quickly."""
+    the queue kernel on a case that ncu can capture quickly.  The launch shape is the library's default (not
+    autotuned) unless --blocks-per-sm / --period say otherwise."""
     import torch
 
     import phoenix_b200 as P
@@ -327,7 +328,8 @@ def run_batch_small(args):
     snap = P.Snapshot.load(dump, grid, nlevels=BATCH["nlevels"])
     imgs = [dict(im, img=256) for im in batch_images()[:args.batch_images]]
     stream = torch.cuda.Stream(device=dev)
-    b = P.Batch([(snap, P.make_params(precision="fp32", **im)) for im in imgs], blocks_per_sm=3, period=32)
+    b = P.Batch([(snap, P.make_params(precision="fp32", **im)) for im in imgs], blocks_per_sm=args.blocks_per_sm,
+                period=args.period)
     ts = []
     for r in range(max(1, args.warmup) + max(1, args.steps)):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -340,7 +342,10 @@ def run_batch_small(args):
     steps = sum(b.result(k)[1]["steps"] for k in range(len(imgs)))
     ms = min(ts[max(1, args.warmup):])
     print(json.dumps({"workload": "batch-small", "images": len(imgs), "ms": ms, "ray_steps": steps,
-                      "ray_steps_per_s": steps / (ms * 1e-3), "tuning": b.tuning()["regs"]}), flush=True)
+                      "ray_steps_per_s": steps / (ms * 1e-3),
+                      "tuning": {k: v for k, v in b.tuning().items()
+                                 if k in ("blocks_per_sm", "period", "refill_lanes", "regs", "grid", "block")}}),
+          flush=True)
     b.close()
     snap.close()
 
