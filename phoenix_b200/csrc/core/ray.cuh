@@ -5,7 +5,7 @@
 // step.  FP64 processes the previous point's sample, as the reference does; the FP32 and mixed paths process this
 // point's (see advance() for why both give the same samples).
 // Because the state is explicit, a warp can retire a finished ray and start a new one in the same lane while its
-// neighbours keep marching (the kernel's lane refill), instead of idling until the warp's longest ray ends.
+// neighbours keep marching (the kernels' partial refill, refill_lanes < 32), as well as refill all its lanes at once.
 //
 // Each mode has two precisions: G of the geodesic (state, RK4, step size, leaf placement) and R of the plasma stage
 // (interpolated fluid, synchrotron coefficients, transfer operator).

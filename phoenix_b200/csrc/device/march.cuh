@@ -1,11 +1,12 @@
-// The fused raymarch kernel: a persistent grid of warps, one ray per lane, with warp-level lane refill.
+// The fused raymarch kernel: a persistent grid of warps, one ray per lane, fed from a device job queue.
 //
 // Every pass of the march loop is one Ray::advance() per live lane (geodesic step + leaf lookups + the plasma
-// stage of the previous sample + its transfer operator for every frequency).  Every `period` passes each warp
-// collects its finished lanes with a ballot, takes that many pixel jobs from the device queue with one atomic,
-// and starts the new rays in those lanes (prefix-popcount ranks), so a warp never waits for its longest ray:
-// the reference kernel (src/device/kernel.cu:70-100) runs each pixel's whole inner loop per lane, and a lane that
-// finished early idles until its warp's longest ray ends.
+// stage of the sample + its transfer operator for every frequency).  A warp collects its finished lanes with a
+// ballot, takes that many pixel jobs from the queue with one atomic and starts the new rays in those lanes
+// (prefix-popcount ranks): when `refill_lanes` of its lanes have finished (checked every 64 passes; by default all
+// 32) or at the end of a `period` of passes.  The reference kernel (src/device/kernel.cu:70-100) gives each thread
+// a fixed share of the pixels; here the grid stays resident and warps take jobs as they free up.  The refill policy
+// is discussed beside kDefaultPeriod below: refilling single lanes as early as possible measured slowest.
 //
 // Device buffers a launch touches: the snapshot pool and job list (read), the FreqOut image (written once per
 // pixel), optional per-pixel statistics, and a 16-word counter block (queue head + diagnostic sums).
