@@ -890,7 +890,9 @@ def main():
                        "precision": args.precision, "images_per_step": len(params), "rays_per_step": len(params) * npix,
                        "l2": "flushed (256 MB write) before every timed step; snapshot 0.5 GB > L2",
                        "parallelism": f"{world} GPU(s), independent replicas",
-                       "pixel_order": order_desc(P, params, args.order)},
+                       "pixel_order": order_desc(P, params, args.order),
+                       "refill": ("whole warp (a warp takes new jobs when all its rays have ended)"
+                                  + (f", or its finished lanes every {args.period} passes" if args.period > 0 else ""))},
             "images_per_s": nimg / (ms_max * 1e-3) * world,
             "rays_per_s": nimg * npix / (ms_max * 1e-3) * world,
             "ray_steps_per_step": steps_total / args.steps,
