@@ -140,6 +140,8 @@ def test_results_independent_of_scheduling(gpu_snapshots, bps):
     default, _ = gpu_snapshots["cfg1"].render(P.make_params(precision="fp32", **kw))
     l1 = np.abs(default[..., :4] - base[..., :4]).sum() / np.abs(base[..., :4]).sum()
     assert l1 <= 1e-5, l1
+    with pytest.raises(P.PhxError, match="refill_lanes"):
+        gpu_snapshots["cfg1"].render(P.make_params(precision="fp32", refill_lanes=33, **kw))
 
 
 @pytest.mark.parametrize("bps", [3, 4])
