@@ -129,8 +129,8 @@ def test_frequencies_are_independent(gpu_snapshots):
 @pytest.mark.parametrize("bps", [0, 1, 4])
 def test_results_independent_of_scheduling(gpu_snapshots, bps):
     """A ray's arithmetic does not depend on which lane, warp or refill round runs it: for one compiled variant the
-    image is bit-identical whatever the refill period or threshold.  Variants compiled for other register caps round differently
-    (separate compilations), so across them the images agree to FP32 rounding."""
+    image is bit-identical whatever the refill period or threshold.  Variants compiled for other register caps round
+    differently (separate compilations), so across them the images agree to FP32 rounding."""
     kw = case_params("cfg1")
     base, _ = gpu_snapshots["cfg1"].render(P.make_params(precision="fp32", blocks_per_sm=bps, period=1, **kw))
     for period, refill in ((4, 0), (16, 0), (64, 1), (256, 8), (1 << 20, 24), (1 << 20, 32)):
