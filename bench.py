@@ -45,12 +45,12 @@ FLOPS = dict(step=3445.0, sample=870.0, freq=1224.0)
 # its job index (4 B) and one 48 B FreqOut record per frequency.
 BYTES = dict(sample=256.0, step=28.0, ray=4.0, ray_freq=48.0)
 # DRAM bytes (read + write) per ray-step of k_march, from an ncu capture of one launch of this workload (the 60 deg
-# image): dram__bytes_read.sum + dram__bytes_write.sum = 803.6 MB over the launch's 726.6M ray-steps.  Scaled to the
-# average launch by its ray-steps.
-DRAM_BYTES_PER_STEP = 1.106
+# image, default job order and refill policy): dram__bytes_read.sum + dram__bytes_write.sum = 773.3 MB over the
+# launch's 726.6M ray-steps.  Scaled to the average launch by its ray-steps.
+DRAM_BYTES_PER_STEP = 1.064
 # FMA-pipe share of active cycles of k_march on this workload (ncu sm__pipe_fma_cycles_active.avg.pct_of_peak_
-# sustained_active, one launch of the 60 deg image).
-FMA_PIPE_ACTIVE = 0.449
+# sustained_active, one launch of the 60 deg image, default job order and refill policy).
+FMA_PIPE_ACTIVE = 0.465
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 
 
