@@ -5,9 +5,9 @@
 // ballot, takes that many pixel jobs from the queue with one atomic and starts the new rays in those lanes
 // (prefix-popcount ranks): when `refill_lanes` of its lanes have finished (checked every 64 passes; by default all
 // 32) or at the end of a `period` of passes.  The reference kernel (src/device/kernel.cu:56-100) runs each pixel's
-// whole inner loop in its lane and grabs jobs per warp, so its lanes too wait for their warp's longest ray; here the
-// loop is resumable pass by pass, which also allows partial refills (refill_lanes < 32).  The refill policy is
-// discussed beside kDefaultPeriod below: refilling single lanes as early as possible measured slowest.
+// whole inner loop in its lane and takes jobs with one atomic per warp; here the loop is resumable pass by pass, so
+// the refill policy is a choice (refill_lanes, period), discussed beside kDefaultPeriod below: refilling single lanes
+// as early as possible measured slowest.
 //
 // Device buffers a launch touches: the snapshot pool and job list (read), the FreqOut image (written once per
 // pixel), optional per-pixel statistics, and a 16-word counter block (queue head + diagnostic sums).
